@@ -1,0 +1,507 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 W-projection gridder on the large single-job
+workload (plain_large: 39,244,800 visibilities onto an 8192^2 complex64
+grid, 256 w-planes with support 4..36, oversample 4, FP32 data, kernels and
+grid, FP64 coordinates).
+
+A step grids the whole job once.  `value` is visibilities per second (Gvis/s)
+with inputs resident in HBM, timed with CUDA events on the launching stream
+over exactly --steps steps after --warmup untimed steps; the inputs (0.8 GB
+per step) are larger than L2, so no flush is needed between steps.  `e2e` is
+the same metric through the drop-in C entry point oskar_grid_wproj_f with
+pinned host buffers (host<->device copies inside the timed region).
+
+Multi-GPU (torchrun, one process per GPU): every rank grids its own
+independent job (different seed) with no collective on the data path; the
+elapsed time is the max over ranks (weak scaling).
+
+--impl reference times the reference's own CPU gridder (oskar_grid_wproj.c
+compiled unmodified into oracle/_ref, driven in its fixed 10000-point calls
+over a bounded random sample of the same workload) on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+METRIC = ("Gvis/s & grid updates/s at ≤1e-5 rel err vs FP64; "
+          "serving p50/p99 latency")
+UNIT = "Gvis/s"
+WORKLOAD_DESC = ("plain_large: 512 stations log-radial to 30 km (130,816 "
+                 "baselines) x 300 samples = 39,244,800 visibilities, 150 MHz, "
+                 "dec -30 deg; grid 8192^2 complex64; 256 w-planes, support "
+                 "4->36, oversample 4, conv_size_half 149; FP32 data/kernels/"
+                 "grid, FP64 coordinates")
+DATA_DESC = ("synthetic: seeded Earth-rotation uvw, 10 point sources + "
+             "complex Gaussian noise, analytic Gaussian x chirp W-kernels")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ---------------------------------------------------------------------------
+# helpers
+# ---------------------------------------------------------------------------
+
+def dist_setup(gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per launch of the gridding kernel from the committed ncu
+    summary (profiles/romein_grid_kernel_plain_large.md), or None."""
+    p = os.path.join(ROOT, "profiles", "romein_grid_kernel_plain_large.md")
+    try:
+        text = open(p).read()
+    except OSError:
+        return None
+    m = re.search(r"dram_bytes_per_launch_full_job:\s*([0-9.eE+]+)", text)
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples every 200 ms while running."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,"
+              "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200", "-i",
+                 str(self.dev)], stdout=open(self.path, "w"),
+                stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap")
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9])
+                          if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def host_threads():
+    try:
+        n = len(os.sched_getaffinity(0))
+    except AttributeError:
+        n = os.cpu_count() or 1
+    return max(1, n)
+
+
+def mem_available_bytes():
+    try:
+        for line in open("/proc/meminfo"):
+            if line.startswith("MemAvailable:"):
+                return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return 16 << 30
+
+
+def ensure_oracle():
+    from oracle import oracle as O
+    if not os.path.exists(O.ORACLE_SO) or (
+            not os.path.exists(O.REF_SO) and
+            os.path.exists("/root/reference/oskar_grid_wproj.c")):
+        O.build()
+    return O
+
+
+def cpu_sample_time(O, wl_host, single, use_reference, target_s, seed,
+                    threads=None):
+    """Time the reference (or the restatement) on a random sample of the
+    workload sized for about target_s seconds on `threads` host threads.
+    Returns (seconds, sample_points, grid_updates, threads, kind)."""
+    n_all = len(wl_host["uu"])
+    g = wl_host["grid_size"]
+    grid_bytes = 2 * g * g * (4 if single else 8)
+    t = threads or host_threads()
+    t = max(1, min(t, int(0.5 * mem_available_bytes() // grid_bytes), 256))
+    rng = np.random.default_rng(seed)
+
+    def sample(m):
+        idx = np.sort(rng.choice(n_all, size=min(m, n_all), replace=False))
+        s = dict(wl_host)
+        for k in ("uu", "vv", "ww", "weight"):
+            s[k] = wl_host[k][idx]
+        s["vis"] = wl_host["vis"].reshape(-1, 2)[idx].reshape(-1)
+        return s
+    # calibrate the per-thread rate on a small sample
+    cal = sample(20000 * t)
+    secs, _, _, _ = O.time_parallel(cal, single, t, use_reference)
+    rate = len(cal["uu"]) / max(secs, 1e-6)
+    m = int(max(10000 * t, rate * target_s))
+    s = sample(m)
+    secs, _, _, _ = O.time_parallel(s, single, t, use_reference)
+    taps = O.count_taps(s)
+    kind = "reference" if use_reference else "port"
+    return secs, len(s["uu"]), taps, t, kind
+
+
+# ---------------------------------------------------------------------------
+# arms
+# ---------------------------------------------------------------------------
+
+def make_workload(rank):
+    from fpga_gridding_b200 import workloads as W
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    wl = W.plain_large(seed=1 + rank, device=dev)
+    return wl.to(dtype=torch.float32)
+
+
+def host_dict(wl32):
+    d = wl32.numpy()
+    d["cell_size_rad"] = float(np.float32(wl32.cell_size_rad))
+    d["w_scale"] = float(np.float32(wl32.w_scale))
+    return d
+
+
+def run_b200(args, world, rank, local):
+    import ctypes as C
+    import fpga_gridding_b200 as fg
+    from fpga_gridding_b200 import _lib
+
+    lib = fg.load()
+    wl = make_workload(rank)
+    n = wl.num_points
+    g = wl.grid_size
+    cell = float(np.float32(wl.cell_size_rad))
+    wsc = float(np.float32(wl.w_scale))
+    ws = fg.Workspace(local)
+    lib.oskar_b200_set_stage_timing(ws.handle, 1)
+    cube = fg.Cube(ws, wl.support, wl.oversample, wl.conv_size_half,
+                   wl.conv_func, data_is_double=False)
+    grid = torch.zeros(2 * g * g, dtype=torch.float32, device="cuda")
+    skip = torch.zeros(1, dtype=torch.int64, device="cuda")
+    norm = torch.zeros(1, dtype=torch.float64, device="cuda")
+    # A real (non-default) stream: the library launches on it and the
+    # timing events are recorded on it.
+    stream = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    opts = fg.options()
+
+    def step():
+        fg.grid_device(ws, cube, wl.uu, wl.vv, wl.ww, wl.vis, wl.weight,
+                       cell, wsc, g, grid, skip, norm, opts=opts,
+                       stream=stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    grid_ms, launches, stats = [], 0, None
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+        stream.synchronize()  # stage events of this step are now readable
+        stats = ws.stats()
+        grid_ms.append(stats.grid_ms)
+        launches += stats.kernel_launches
+        if stats.status != 0:
+            raise RuntimeError(f"device check status {stats.status}")
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    elapsed_ms = ev0.elapsed_time(ev1)
+    barrier(world)
+    elapsed_ms = max_over_ranks(elapsed_ms, world)
+    ms_per_step = elapsed_ms / args.steps
+    total_vis = n * args.steps * world
+    value = total_vis / (elapsed_ms * 1e-3) / 1e9
+    updates = stats.grid_updates
+    updates_per_s = updates * args.steps * world / (elapsed_ms * 1e-3)
+
+    # Roofline of the dominant kernel (the Romein gridding kernel).
+    kernel_ms = statistics.mean(grid_ms)
+    cube_slab_bytes = cube.bytes
+    alg_bytes = n * (16 + 8) + 2 * g * g * 8 + cube_slab_bytes
+    achieved = alg_bytes / (kernel_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = profiled_traffic()
+    roofline = {"kernel": "romein_grid_kernel<float,float2,L1>", "bound": "hbm",
+                "achieved": round(achieved, 2), "peak": peak,
+                "peak_source": peak_kind, "unit": "GB/s",
+                "frac": round(achieved / peak, 4),
+                "traffic": traffic,
+                "algorithmic_bytes_per_launch": alg_bytes,
+                "kernel_ms": round(kernel_ms, 3)}
+    # L2-atomic roofline: measured complex-FP32 red.v2 rate on an
+    # L2-resident 2048^2 grid.
+    rate = C.c_double(0.0)
+    probe = torch.zeros(2 * 2048 * 2048, dtype=torch.float32, device="cuda")
+    _lib.check(lib.oskar_b200_measure_atomic_rate(
+        ws.handle, C.c_void_p(probe.data_ptr()), 2048, 2000, C.byref(rate)))
+    del probe
+    kernel_updates_per_s = updates / (kernel_ms * 1e-3)
+    l2_atomic = {"peak_red_v2_per_s": rate.value,
+                 "grid_updates_per_s_in_kernel": kernel_updates_per_s,
+                 "frac": round(kernel_updates_per_s / rate.value, 4),
+                 "issued_atomics_per_launch": stats.atomic_flushes,
+                 "issued_atomic_frac": round(
+                     stats.atomic_flushes / (kernel_ms * 1e-3) / rate.value, 4)}
+    stage_ms = {"prep": round(stats.prep_ms, 3), "sort": round(stats.sort_ms, 3),
+                "permute_tasks": round(stats.tasks_ms, 3),
+                "grid": round(stats.grid_ms, 3)}
+
+    # End to end through the drop-in C entry point with pinned host buffers.
+    e2e = run_e2e(args, wl, world)
+
+    out = {"metric": METRIC, "value": round(value, 4), "unit": UNIT,
+           "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": round(ms_per_step, 3), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": DATA_DESC,
+           "config": {"workload": WORKLOAD_DESC, "num_points": n,
+                      "grid_size": g, "num_w_planes": wl.num_w_planes,
+                      "oversample": wl.oversample,
+                      "parallelism": f"replicas x{world}" if world > 1 else "single",
+                      "l2": "inputs (0.8 GB/step) larger than L2; no flush"},
+           "grid_updates_per_s": updates_per_s,
+           "grid_updates_per_step": updates,
+           "roofline": roofline, "l2_atomic": l2_atomic, "stage_ms": stage_ms,
+           "e2e": e2e, "gpu_launches": launches, "clocks": clk}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = run_cpu_baseline(args, wl)
+        out["rel_err_vs_fp64"] = audit_error(wl)
+    return out
+
+
+def run_e2e(args, wl, world):
+    """Drop-in oskar_grid_wproj_f on pinned host buffers, K steps."""
+    import fpga_gridding_b200 as fg
+    pin = lambda t: t.cpu().pin_memory()
+    h = {k: pin(getattr(wl, k)) for k in ("uu", "vv", "ww", "vis", "weight",
+                                          "conv_func")}
+    g = wl.grid_size
+    hgrid = torch.zeros(2 * g * g, dtype=torch.float32).pin_memory()
+    a = {k: v.numpy() for k, v in h.items()}
+    gridn = hgrid.numpy()
+    cell = float(np.float32(wl.cell_size_rad))
+    wsc = float(np.float32(wl.w_scale))
+
+    def call():
+        return fg.oskar_grid_wproj_f(
+            wl.num_w_planes, wl.support, wl.oversample, wl.conv_size_half,
+            a["conv_func"], wl.num_points, a["uu"], a["vv"], a["ww"],
+            a["vis"], a["weight"], cell, wsc, g, 0.0, gridn)
+    for _ in range(max(1, args.warmup)):
+        call()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        call()
+    secs = time.perf_counter() - t0
+    secs = max_over_ranks(secs, world)
+    n = wl.num_points
+    h2d = n * 5 * 4 + a["conv_func"].nbytes + gridn.nbytes + wl.num_w_planes * 4
+    d2h = gridn.nbytes + 16
+    fg.load().oskar_grid_wproj_b200_release_thread_cache()
+    return {"value": round(n * args.steps * world / secs / 1e9, 4),
+            "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h,
+            "ms_per_step": round(1e3 * secs / args.steps, 3),
+            "path": "oskar_grid_wproj_f (drop-in C ABI), pinned host buffers"}
+
+
+def run_cpu_baseline(args, wl):
+    O = ensure_oracle()
+    use_ref = O.reference_lib() is not None
+    hd = host_dict(wl)
+    secs, m, taps, t, kind = cpu_sample_time(O, hd, True, use_ref,
+                                             args.cpu_seconds, seed=99)
+    return {"value": round(m / secs / 1e9, 6), "unit": UNIT, "cores": t,
+            "kind": kind, "grid_updates_per_s": taps / secs,
+            "sample": (f"{m} visibilities drawn uniformly (seeded) from the "
+                       f"39,244,800 of the workload; "
+                       + ("reference oskar_grid_wproj_f compiled unmodified, "
+                          "driven in its fixed 10000-point calls"
+                          if kind == "reference" else
+                          "C restatement of oskar_grid_wproj_f")
+                       + f"; {t} threads with private 8192^2 grids; "
+                       f"{secs:.2f} s")}
+
+
+def audit_error(wl, m=200000):
+    """Relative RMS of the GPU grid vs the FP64 oracle on a seeded sample."""
+    import fpga_gridding_b200 as fg
+    O = ensure_oracle()
+    hd = host_dict(wl)
+    rng = np.random.default_rng(7)
+    idx = np.sort(rng.choice(len(hd["uu"]), size=m, replace=False))
+    s = dict(hd)
+    for k in ("uu", "vv", "ww", "weight"):
+        s[k] = hd[k][idx]
+    s["vis"] = hd["vis"].reshape(-1, 2)[idx].reshape(-1)
+    sd = dict(s)
+    for k in ("conv_func", "uu", "vv", "ww", "vis", "weight"):
+        sd[k] = np.asarray(s[k], np.float64)
+    _, n_ref, g_ref = O.grid_d(sd, threads=host_threads())
+    _, n_gpu, g_gpu = fg.grid_workload(s, single=True)
+    fg.load().oskar_grid_wproj_b200_release_thread_cache()
+    return {"grid_rel_rms": O.rel_rms(g_gpu, g_ref),
+            "norm_rel": abs(n_gpu - n_ref) / abs(n_ref),
+            "sample": f"{m} seeded visibilities of the workload, FP32 drop-in "
+                      "vs FP64 oracle on the same inputs"}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return None
+    O = ensure_oracle()
+    use_ref = O.reference_lib() is not None
+    wl = make_workload(0)
+    hd = host_dict(wl)
+    del wl
+    torch.cuda.empty_cache() if torch.cuda.is_available() else None
+    per_step_s = max(2.0, min(10.0, 120.0 / max(1, args.steps + args.warmup)))
+    tot_secs, tot_m, tot_taps, t, kind = 0.0, 0, 0, 1, "port"
+    for i in range(args.warmup + args.steps):
+        secs, m, taps, t, kind = cpu_sample_time(O, hd, True, use_ref,
+                                                 per_step_s, seed=1000 + i)
+        if i >= args.warmup:
+            tot_secs += secs
+            tot_m += m
+            tot_taps += taps
+    value = tot_m / tot_secs / 1e9
+    desc = ("reference oskar_grid_wproj_f (oskar_grid_wproj.c compiled "
+            "unmodified), driven in its fixed 10000-point calls"
+            if kind == "reference" else "C restatement of oskar_grid_wproj_f")
+    return {"impl": "reference", "metric": METRIC, "value": round(value, 6),
+            "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(1e3 * tot_secs / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": DATA_DESC,
+            "config": {"workload": WORKLOAD_DESC,
+                       "num_points": len(hd["uu"]),
+                       "grid_size": hd["grid_size"]},
+            "grid_updates_per_s": tot_taps / tot_secs,
+            "cpu_baseline": {"value": round(value, 6), "unit": UNIT,
+                             "cores": t, "kind": kind,
+                             "sample": f"each step: about {per_step_s:.0f} s "
+                                       f"of a seeded uniform sample of the "
+                                       f"workload's visibilities; {desc}; "
+                                       f"{t} threads with private grids"},
+            "e2e": {"value": round(value, 6), "unit": UNIT,
+                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    ap.add_argument("--cpu-seconds", type=float, default=8.0,
+                    help="target wall time of the CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        # CPU only: rank 0 runs, the other ranks exit without work.
+        rank = int(os.environ.get("RANK", "0"))
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        out = run_reference(args, world, rank)
+        if out is not None:
+            print(json.dumps(out), flush=True)
+        return
+    world, rank, local = dist_setup(args.gpus)
+    try:
+        out = run_b200(args, world, rank, local)
+        if rank == 0 and out is not None:
+            print(json.dumps(out), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,12 @@
+"""B200-native W-projection gridder (drop-in for the reference's
+oskar_grid_wproj_d / oskar_grid_wproj_f).
+
+The product is the C-ABI library libgridder_b200.so (hand-written sm_100a
+CUDA, declared in include/oskar_grid_wproj_b200.h); this package is its
+Python front end.  Importing the package does not load the library;
+calling any gridding function does, and fails loudly if it is missing.
+"""
+from ._lib import EXPORTED_SYMBOLS, GridderError, LIB_PATH, load  # noqa: F401
+from .gridder import (Cube, Workspace, grid_device, grid_workload,  # noqa: F401
+                      options, oskar_grid_wproj_d, oskar_grid_wproj_f,
+                      place_device)

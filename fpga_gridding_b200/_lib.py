@@ -1,0 +1,141 @@
+"""ctypes binding of libgridder_b200.so (the C ABI in
+include/oskar_grid_wproj_b200.h).  Loading fails loudly when the library
+has not been built: there is no CPU fallback."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgridder_b200.so")
+
+# Every symbol include/oskar_grid_wproj_b200.h declares.
+EXPORTED_SYMBOLS = (
+    "oskar_grid_wproj_d",
+    "oskar_grid_wproj_f",
+    "oskar_grid_wproj_b200_last_error",
+    "oskar_grid_wproj_b200_error_string",
+    "oskar_grid_wproj_b200_release_thread_cache",
+    "oskar_b200_options_init",
+    "oskar_b200_workspace_create",
+    "oskar_b200_workspace_free",
+    "oskar_b200_workspace_bytes",
+    "oskar_b200_cube_create",
+    "oskar_b200_cube_free",
+    "oskar_b200_cube_bytes",
+    "oskar_b200_grid",
+    "oskar_b200_fold_compensation",
+    "oskar_b200_place",
+    "oskar_b200_last_stats",
+    "oskar_b200_set_stage_timing",
+    "oskar_b200_measure_atomic_rate",
+    "oskar_b200_build_info",
+)
+
+# Status codes (oskar_B200Status).
+OK = 0
+ERR_INVALID_ARGUMENT = 1
+ERR_NO_DEVICE = 2
+ERR_OUT_OF_MEMORY = 3
+ERR_CUDA = 4
+ERR_UNSUPPORTED = 5
+ERR_DEVICE_CHECK = 6
+ERR_TIMEOUT = 7
+ERR_OVER_BUDGET = 8
+
+COORDS_F64 = 0
+COORDS_REFERENCE_F32 = 1
+KERNEL_NATIVE = 0
+KERNEL_F16 = 1
+KERNEL_BF16 = 2
+ACCUM_PLAIN = 0
+ACCUM_COMPENSATED = 1
+
+
+class Options(C.Structure):
+    _fields_ = [("coord_mode", C.c_int), ("kernel_type", C.c_int),
+                ("accum_mode", C.c_int), ("apply_weight", C.c_int),
+                ("classes_per_thread", C.c_int), ("staging", C.c_int),
+                ("reserved", C.c_int * 10)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("num_points", C.c_ulonglong), ("num_gridded", C.c_ulonglong),
+                ("grid_updates", C.c_ulonglong), ("num_tasks", C.c_ulonglong),
+                ("atomic_flushes", C.c_ulonglong), ("status", C.c_int),
+                ("kernel_launches", C.c_int), ("prep_ms", C.c_float),
+                ("sort_ms", C.c_float), ("tasks_ms", C.c_float),
+                ("grid_ms", C.c_float)]
+
+
+_P = C.c_void_p
+_SZ = C.c_size_t
+_lib = None
+
+
+def load():
+    """The gridder library (raises RuntimeError if it is not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"{LIB_PATH} is missing: build it with "
+            "`make -C fpga_gridding_b200/csrc` (or __graft_entry__.build())")
+    lib = C.CDLL(LIB_PATH)
+    grid_common = [_SZ, _P, C.c_int, C.c_int, _P, _SZ, _P, _P, _P, _P, _P]
+    lib.oskar_grid_wproj_d.argtypes = grid_common + [
+        C.c_double, C.c_double, C.c_int, _P, _P, _P]
+    lib.oskar_grid_wproj_f.argtypes = grid_common + [
+        C.c_float, C.c_float, C.c_int, _P, _P, _P]
+    lib.oskar_grid_wproj_d.restype = lib.oskar_grid_wproj_f.restype = None
+    lib.oskar_grid_wproj_b200_last_error.restype = C.c_int
+    lib.oskar_grid_wproj_b200_error_string.argtypes = [C.c_int]
+    lib.oskar_grid_wproj_b200_error_string.restype = C.c_char_p
+    lib.oskar_grid_wproj_b200_release_thread_cache.restype = None
+    lib.oskar_b200_options_init.argtypes = [C.POINTER(Options)]
+    lib.oskar_b200_options_init.restype = None
+    lib.oskar_b200_workspace_create.argtypes = [C.c_int, C.POINTER(_P)]
+    lib.oskar_b200_workspace_free.argtypes = [_P]
+    lib.oskar_b200_workspace_bytes.argtypes = [_P]
+    lib.oskar_b200_workspace_bytes.restype = _SZ
+    lib.oskar_b200_cube_create.argtypes = [
+        _P, _SZ, _P, C.c_int, C.c_int, _P, C.c_int, C.c_int, C.c_int,
+        C.c_int, _P, C.POINTER(_P)]
+    lib.oskar_b200_cube_free.argtypes = [_P]
+    lib.oskar_b200_cube_bytes.argtypes = [_P]
+    lib.oskar_b200_cube_bytes.restype = _SZ
+    lib.oskar_b200_grid.argtypes = [
+        _P, _P, C.POINTER(Options), _SZ, _P, _P, _P, _P, _P, C.c_double,
+        C.c_double, C.c_int, _P, _P, _P, _P]
+    lib.oskar_b200_fold_compensation.argtypes = [_P, _P, C.c_int, _P]
+    lib.oskar_b200_place.argtypes = [
+        _P, C.c_int, C.c_int, _SZ, _P, C.c_int, _SZ, _P, _P, _P, C.c_double,
+        C.c_double, C.c_int] + [_P] * 7 + [_P]
+    lib.oskar_b200_last_stats.argtypes = [_P, C.POINTER(Stats)]
+    lib.oskar_b200_build_info.restype = C.c_char_p
+    lib.oskar_b200_set_stage_timing.argtypes = [_P, C.c_int]
+    lib.oskar_b200_measure_atomic_rate.argtypes = [
+        _P, _P, C.c_int, C.c_int, C.POINTER(C.c_double)]
+    for name in ("oskar_b200_workspace_create", "oskar_b200_workspace_free",
+                 "oskar_b200_cube_create", "oskar_b200_cube_free",
+                 "oskar_b200_grid", "oskar_b200_fold_compensation",
+                 "oskar_b200_place", "oskar_b200_last_stats",
+                 "oskar_b200_set_stage_timing",
+                 "oskar_b200_measure_atomic_rate"):
+        getattr(lib, name).restype = C.c_int
+    _lib = lib
+    return lib
+
+
+class GridderError(RuntimeError):
+    def __init__(self, status: int, where: str = ""):
+        msg = load().oskar_grid_wproj_b200_error_string(status).decode()
+        super().__init__(f"{where}: status {status} ({msg})" if where else
+                         f"status {status} ({msg})")
+        self.status = status
+
+
+def check(status: int, where: str = "") -> None:
+    if status != OK:
+        raise GridderError(status, where)

@@ -1,0 +1,617 @@
+// Public C ABI of the B200 gridder: the drop-in oskar_grid_wproj_{d,f}
+// replacements and the extended device-resident API.
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <vector>
+
+#include "common.cuh"
+#include "internal.h"
+
+#define B200_STR2(x) #x
+#define B200_STR(x) B200_STR2(x)
+
+using namespace b200;
+
+namespace {
+
+thread_local int tls_status = OSKAR_B200_OK;
+
+// Makes `device` current for the scope of a call and restores the caller's.
+struct DeviceGuard
+{
+    int prev = -1;
+    bool changed = false;
+    explicit DeviceGuard(int device)
+    {
+        if (cudaGetDevice(&prev) == cudaSuccess && prev != device)
+            changed = cudaSetDevice(device) == cudaSuccess;
+    }
+    ~DeviceGuard()
+    {
+        if (changed) cudaSetDevice(prev);
+    }
+};
+
+// The caller's current device, if it is a usable sm_100 device.
+int current_device(int* device)
+{
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+    {
+        cudaGetLastError();
+        return OSKAR_B200_ERR_NO_DEVICE;
+    }
+    if (cudaGetDevice(device) != cudaSuccess) return OSKAR_B200_ERR_NO_DEVICE;
+    int major = 0;
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, *device);
+    // The kernels are built for sm_100a only.
+    if (major != 10) return OSKAR_B200_ERR_NO_DEVICE;
+    return OSKAR_B200_OK;
+}
+
+int workspace_create(int device, oskar_B200Workspace** out)
+{
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 ||
+        device >= count)
+    {
+        cudaGetLastError();
+        return OSKAR_B200_ERR_NO_DEVICE;
+    }
+    int major = 0;
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device);
+    if (major != 10) return OSKAR_B200_ERR_NO_DEVICE;
+    DeviceGuard g(device);
+    auto* ws = new (std::nothrow) oskar_B200Workspace();
+    if (!ws) return OSKAR_B200_ERR_OUT_OF_MEMORY;
+    ws->device = device;
+    int smem = 0;
+    cudaDeviceGetAttribute(&ws->num_sms, cudaDevAttrMultiProcessorCount, device);
+    cudaDeviceGetAttribute(&smem, cudaDevAttrMaxSharedMemoryPerBlockOptin,
+                           device);
+    ws->smem_optin = (size_t)smem;
+    cudaError_t e = cudaStreamCreateWithFlags(&ws->stream,
+                                              cudaStreamNonBlocking);
+    if (e == cudaSuccess)
+        e = cudaMallocHost(&ws->h_counters,
+                           sizeof(unsigned long long) * CNT_COUNT);
+    if (e != cudaSuccess)
+    {
+        if (ws->stream) cudaStreamDestroy(ws->stream);
+        delete ws;
+        cudaGetLastError();
+        return status_from_cuda(e);
+    }
+    memset(ws->h_counters, 0, sizeof(unsigned long long) * CNT_COUNT);
+    *out = ws;
+    return OSKAR_B200_OK;
+}
+
+void workspace_free(oskar_B200Workspace* ws)
+{
+    if (!ws) return;
+    DeviceGuard g(ws->device);
+    if (ws->stream) cudaStreamSynchronize(ws->stream);
+    for (cudaEvent_t& e : ws->events)
+        if (e) cudaEventDestroy(e);
+    if (ws->h_counters) cudaFreeHost(ws->h_counters);
+    if (ws->stream) cudaStreamDestroy(ws->stream);
+    delete ws;  // DeviceBuffer destructors free device memory
+}
+
+// Per-thread cache of the drop-in path: a workspace for the current device
+// and a cube object whose device buffers are reused across calls.
+struct ThreadCache
+{
+    oskar_B200Workspace* ws = nullptr;
+    oskar_B200Cube* cube = nullptr;
+    void release()
+    {
+        if (ws)
+        {
+            DeviceGuard g(ws->device);
+            delete cube;
+            workspace_free(ws);
+        }
+        else
+        {
+            delete cube;
+        }
+        ws = nullptr;
+        cube = nullptr;
+    }
+    ~ThreadCache() { release(); }
+};
+thread_local ThreadCache tls_cache;
+
+int validate_cube_args(size_t num_w_planes, const int* support,
+                       int oversample, int conv_size_half,
+                       const void* conv_func)
+{
+    if (num_w_planes == 0 || num_w_planes > (1u << 15) || !support ||
+        !conv_func || oversample < 1 || oversample > 64 ||
+        conv_size_half < 1)
+        return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    const long long csh = conv_size_half;
+    const long long total = (long long)num_w_planes * csh * csh;
+    const int half = (oversample + 1) / 2;
+    for (size_t p = 0; p < num_w_planes; ++p)
+    {
+        const long long s = support[p];
+        if (s < 0 || s > 4096) return OSKAR_B200_ERR_INVALID_ARGUMENT;
+        // Largest flat index the reference reads on this plane
+        // (oskar_grid_wproj.c:110-116) must lie inside the cube.
+        const long long e = oversample * s + half;
+        if ((long long)p * csh * csh + e * csh + e >= total)
+            return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    }
+    return OSKAR_B200_OK;
+}
+
+// Builds (or rebuilds) `cube` in place from a device copy of the cube.
+int cube_init(oskar_B200Cube* c, int device, size_t num_w_planes,
+              const int* support, int oversample, int conv_size_half,
+              const void* d_conv, int conv_is_double, int data_is_double,
+              int kernel_type, cudaStream_t st)
+{
+    c->device = device;
+    c->num_planes = (int)num_w_planes;
+    c->oversample = oversample;
+    c->half = (oversample + 1) / 2;
+    c->conv_size_half = conv_size_half;
+    c->data_is_double = data_is_double;
+    c->kernel_type = kernel_type;
+    if (data_is_double)
+        c->elem_bytes = 16;
+    else
+        c->elem_bytes = kernel_type == OSKAR_B200_KERNEL_NATIVE ? 8 : 4;
+    c->planes.assign(num_w_planes, PlaneDesc{});
+    c->max_support = 0;
+    for (size_t p = 0; p < num_w_planes; ++p)
+    {
+        c->planes[p].support = support[p];
+        if (support[p] > c->max_support) c->max_support = support[p];
+    }
+    cudaError_t e = c->d_support.ensure(sizeof(int) * num_w_planes);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(c->d_support.ptr, support,
+                            sizeof(int) * num_w_planes,
+                            cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return status_from_cuda(e);
+    return cube_build(c, d_conv, conv_is_double, st);
+}
+
+int check_options(const oskar_B200Options* opt, int data_is_double)
+{
+    if (opt->coord_mode != OSKAR_B200_COORDS_F64 &&
+        opt->coord_mode != OSKAR_B200_COORDS_REFERENCE_F32)
+        return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    if (data_is_double && opt->coord_mode != OSKAR_B200_COORDS_F64)
+        return OSKAR_B200_ERR_UNSUPPORTED;
+    if (opt->accum_mode != OSKAR_B200_ACCUM_PLAIN)
+        return OSKAR_B200_ERR_UNSUPPORTED;
+    if (opt->staging < 0 || opt->staging > 2)
+        return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    return OSKAR_B200_OK;
+}
+
+int check_grid_args(size_t num_points, const void* uu, const void* vv,
+                    const void* ww, const void* vis, const void* weight,
+                    int apply_weight, int grid_size, const void* grid)
+{
+    if (grid_size < 1 || grid_size > 65535 || !grid)
+        return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    if (num_points >= 0xffffffffull) return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    if (num_points && (!uu || !vv || !ww || !vis))
+        return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    if (num_points && apply_weight && !weight)
+        return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    return OSKAR_B200_OK;
+}
+
+// Reads the device status word copied back by run_grid (after a sync).
+int device_check_status(const oskar_B200Workspace* ws)
+{
+    const unsigned long long s =
+        static_cast<const unsigned long long*>(ws->h_counters)[CNT_STATUS];
+    if (!s) return OSKAR_B200_OK;
+    if (s & DEV_ERR_TIMEOUT) return OSKAR_B200_ERR_TIMEOUT;
+    return OSKAR_B200_ERR_DEVICE_CHECK;
+}
+
+template <typename T>
+int drop_in(size_t num_w_planes, const int* support, int oversample,
+            int conv_size_half, const T* conv_func, size_t num_points,
+            const T* uu, const T* vv, const T* ww, const T* vis,
+            double cell_size_rad, double w_scale, int grid_size,
+            size_t* num_skipped, double* norm, T* grid)
+{
+    const bool dbl = sizeof(T) == sizeof(double);
+    if (!num_skipped || !norm || !grid) return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    int st = validate_cube_args(num_w_planes, support, oversample,
+                                conv_size_half, conv_func);
+    if (st) return st;
+    st = check_grid_args(num_points, uu, vv, ww, vis, nullptr, 0, grid_size,
+                         grid);
+    if (st) return st;
+    int device = 0;
+    st = current_device(&device);
+    if (st) return st;
+    ThreadCache& tc = tls_cache;
+    if (tc.ws && tc.ws->device != device) tc.release();
+    if (!tc.ws)
+    {
+        st = workspace_create(device, &tc.ws);
+        if (st) return st;
+    }
+    if (!tc.cube)
+    {
+        tc.cube = new (std::nothrow) oskar_B200Cube();
+        if (!tc.cube) return OSKAR_B200_ERR_OUT_OF_MEMORY;
+    }
+    oskar_B200Workspace* ws = tc.ws;
+    cudaStream_t s = ws->stream;
+    const size_t n = num_points;
+    const size_t cube_elems = num_w_planes * (size_t)conv_size_half *
+                              conv_size_half * 2;
+    const size_t grid_elems = 2 * (size_t)grid_size * grid_size;
+#define B200_CHECK(expr)                                            \
+    do {                                                            \
+        const cudaError_t e_ = (expr);                              \
+        if (e_ != cudaSuccess) { cudaStreamSynchronize(s);          \
+                                 cudaGetLastError();                \
+                                 return status_from_cuda(e_); }     \
+    } while (0)
+    B200_CHECK(ws->in_cube.ensure(cube_elems * sizeof(T)));
+    B200_CHECK(ws->in_grid.ensure(grid_elems * sizeof(T)));
+    B200_CHECK(ws->in_norm.ensure(2 * sizeof(double)));
+    if (n)
+    {
+        B200_CHECK(ws->in_uu.ensure(n * sizeof(T)));
+        B200_CHECK(ws->in_vv.ensure(n * sizeof(T)));
+        B200_CHECK(ws->in_ww.ensure(n * sizeof(T)));
+        B200_CHECK(ws->in_vis.ensure(2 * n * sizeof(T)));
+        B200_CHECK(cudaMemcpyAsync(ws->in_uu.ptr, uu, n * sizeof(T),
+                                   cudaMemcpyHostToDevice, s));
+        B200_CHECK(cudaMemcpyAsync(ws->in_vv.ptr, vv, n * sizeof(T),
+                                   cudaMemcpyHostToDevice, s));
+        B200_CHECK(cudaMemcpyAsync(ws->in_ww.ptr, ww, n * sizeof(T),
+                                   cudaMemcpyHostToDevice, s));
+        B200_CHECK(cudaMemcpyAsync(ws->in_vis.ptr, vis, 2 * n * sizeof(T),
+                                   cudaMemcpyHostToDevice, s));
+    }
+    B200_CHECK(cudaMemcpyAsync(ws->in_cube.ptr, conv_func,
+                               cube_elems * sizeof(T),
+                               cudaMemcpyHostToDevice, s));
+    B200_CHECK(cudaMemcpyAsync(ws->in_grid.ptr, grid, grid_elems * sizeof(T),
+                               cudaMemcpyHostToDevice, s));
+    B200_CHECK(cudaMemsetAsync(ws->in_norm.ptr, 0, 2 * sizeof(double), s));
+    st = cube_init(tc.cube, device, num_w_planes, support, oversample,
+                   conv_size_half, ws->in_cube.ptr, dbl, dbl,
+                   OSKAR_B200_KERNEL_NATIVE, s);
+    if (st) { cudaStreamSynchronize(s); cudaGetLastError(); return st; }
+    oskar_B200Options opt;
+    oskar_b200_options_init(&opt);
+    double* d_norm = static_cast<double*>(ws->in_norm.ptr);
+    unsigned long long* d_skip =
+        reinterpret_cast<unsigned long long*>(d_norm + 1);
+    st = run_grid(ws, tc.cube, &opt, n, ws->in_uu.ptr, ws->in_vv.ptr,
+                  ws->in_ww.ptr, ws->in_vis.ptr, nullptr, cell_size_rad,
+                  w_scale, grid_size, ws->in_grid.ptr, d_skip, d_norm, s);
+    if (st) { cudaStreamSynchronize(s); cudaGetLastError(); return st; }
+    // Check the job before touching the caller's grid and norm.
+    B200_CHECK(cudaStreamSynchronize(s));
+    B200_CHECK(cudaGetLastError());
+    st = device_check_status(ws);
+    if (st) return st;
+    double out[2];
+    B200_CHECK(cudaMemcpyAsync(out, d_norm, sizeof(out),
+                               cudaMemcpyDeviceToHost, s));
+    B200_CHECK(cudaMemcpyAsync(grid, ws->in_grid.ptr, grid_elems * sizeof(T),
+                               cudaMemcpyDeviceToHost, s));
+    B200_CHECK(cudaStreamSynchronize(s));
+#undef B200_CHECK
+    unsigned long long skipped;
+    memcpy(&skipped, &out[1], sizeof(skipped));
+    *norm += out[0];
+    *num_skipped = (size_t)skipped;
+    return OSKAR_B200_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Drop-in entry points
+// ---------------------------------------------------------------------------
+extern "C" {
+
+void oskar_grid_wproj_d(const size_t num_w_planes, const int* support,
+                        const int oversample, const int conv_size_half,
+                        const double* conv_func, const size_t num_points,
+                        const double* uu, const double* vv, const double* ww,
+                        const double* vis, const double* weight,
+                        const double cell_size_rad, const double w_scale,
+                        const int grid_size, size_t* num_skipped,
+                        double* norm, double* grid)
+{
+    (void)weight;  // ignored, as in oskar_grid_wproj.c:80-81
+    tls_status = drop_in<double>(num_w_planes, support, oversample,
+                                 conv_size_half, conv_func, num_points, uu,
+                                 vv, ww, vis, cell_size_rad, w_scale,
+                                 grid_size, num_skipped, norm, grid);
+}
+
+void oskar_grid_wproj_f(const size_t num_w_planes, const int* support,
+                        const int oversample, const int conv_size_half,
+                        const float* conv_func, const size_t num_points,
+                        const float* uu, const float* vv, const float* ww,
+                        const float* vis, const float* weight,
+                        const float cell_size_rad, const float w_scale,
+                        const int grid_size, size_t* num_skipped,
+                        double* norm, float* grid)
+{
+    (void)weight;  // ignored, as in oskar_grid_wproj.c:184-185
+    tls_status = drop_in<float>(num_w_planes, support, oversample,
+                                conv_size_half, conv_func, num_points, uu, vv,
+                                ww, vis, (double)cell_size_rad,
+                                (double)w_scale, grid_size, num_skipped, norm,
+                                grid);
+}
+
+int oskar_grid_wproj_b200_last_error(void) { return tls_status; }
+
+const char* oskar_grid_wproj_b200_error_string(int status)
+{
+    switch (status)
+    {
+    case OSKAR_B200_OK: return "ok";
+    case OSKAR_B200_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case OSKAR_B200_ERR_NO_DEVICE: return "no usable sm_100 CUDA device";
+    case OSKAR_B200_ERR_OUT_OF_MEMORY: return "out of memory";
+    case OSKAR_B200_ERR_CUDA: return "CUDA runtime error";
+    case OSKAR_B200_ERR_UNSUPPORTED: return "unsupported option combination";
+    case OSKAR_B200_ERR_DEVICE_CHECK: return "device-side bounds check failed";
+    case OSKAR_B200_ERR_TIMEOUT: return "bounded device wait expired";
+    case OSKAR_B200_ERR_OVER_BUDGET: return "job exceeds the memory budget";
+    default: return "unknown status";
+    }
+}
+
+void oskar_grid_wproj_b200_release_thread_cache(void) { tls_cache.release(); }
+
+// ---------------------------------------------------------------------------
+// Extended API
+// ---------------------------------------------------------------------------
+
+void oskar_b200_options_init(oskar_B200Options* opt)
+{
+    if (!opt) return;
+    memset(opt, 0, sizeof(*opt));
+    opt->coord_mode = OSKAR_B200_COORDS_F64;
+    opt->kernel_type = OSKAR_B200_KERNEL_NATIVE;
+    opt->accum_mode = OSKAR_B200_ACCUM_PLAIN;
+}
+
+int oskar_b200_workspace_create(int device, oskar_B200Workspace** ws)
+{
+    if (!ws) return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    return workspace_create(device, ws);
+}
+
+int oskar_b200_workspace_free(oskar_B200Workspace* ws)
+{
+    workspace_free(ws);
+    return OSKAR_B200_OK;
+}
+
+size_t oskar_b200_workspace_bytes(const oskar_B200Workspace* ws)
+{
+    if (!ws) return 0;
+    const DeviceBuffer* bufs[] = {
+        &ws->keys[0], &ws->keys[1], &ws->vals[0], &ws->vals[1], &ws->rec,
+        &ws->srec, &ws->svis, &ws->scan_tmp, &ws->flags, &ws->task_start,
+        &ws->counters, &ws->partials, &ws->plane_counts, &ws->in_uu,
+        &ws->in_vv, &ws->in_ww, &ws->in_vis, &ws->in_weight, &ws->in_grid,
+        &ws->in_cube, &ws->in_norm, &ws->comp_grid};
+    size_t t = 0;
+    for (const DeviceBuffer* b : bufs) t += b->bytes;
+    return t;
+}
+
+int oskar_b200_cube_create(oskar_B200Workspace* ws, size_t num_w_planes,
+                           const int* support, int oversample,
+                           int conv_size_half, const void* conv_func,
+                           int conv_func_is_double, int conv_func_on_device,
+                           int data_is_double, int kernel_type, void* stream,
+                           oskar_B200Cube** cube)
+{
+    if (!ws || !cube) return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    *cube = nullptr;
+    int st = validate_cube_args(num_w_planes, support, oversample,
+                                conv_size_half, conv_func);
+    if (st) return st;
+    if (kernel_type < OSKAR_B200_KERNEL_NATIVE ||
+        kernel_type > OSKAR_B200_KERNEL_BF16)
+        return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    if (data_is_double && kernel_type != OSKAR_B200_KERNEL_NATIVE)
+        return OSKAR_B200_ERR_UNSUPPORTED;
+    DeviceGuard g(ws->device);
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ws->stream;
+    auto* c = new (std::nothrow) oskar_B200Cube();
+    if (!c) return OSKAR_B200_ERR_OUT_OF_MEMORY;
+    const size_t bytes = num_w_planes * (size_t)conv_size_half *
+                         conv_size_half * 2 *
+                         (conv_func_is_double ? sizeof(double) : sizeof(float));
+    const void* d_conv = conv_func;
+    DeviceBuffer staging;
+    if (!conv_func_on_device)
+    {
+        cudaError_t e = staging.ensure(bytes);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(staging.ptr, conv_func, bytes,
+                                cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) { delete c; return status_from_cuda(e); }
+        d_conv = staging.ptr;
+    }
+    st = cube_init(c, ws->device, num_w_planes, support, oversample,
+                   conv_size_half, d_conv, conv_func_is_double,
+                   data_is_double, kernel_type, s);
+    // The staging copy must outlive the kernels that read it.
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (!st && e != cudaSuccess) st = status_from_cuda(e);
+    if (st) { delete c; return st; }
+    *cube = c;
+    return OSKAR_B200_OK;
+}
+
+int oskar_b200_cube_free(oskar_B200Cube* cube)
+{
+    if (!cube) return OSKAR_B200_OK;
+    DeviceGuard g(cube->device);
+    delete cube;
+    return OSKAR_B200_OK;
+}
+
+size_t oskar_b200_cube_bytes(const oskar_B200Cube* cube)
+{
+    if (!cube) return 0;
+    return cube->d_slabs.bytes + cube->d_planes.bytes +
+           cube->d_norm_table.bytes + cube->d_support.bytes;
+}
+
+int oskar_b200_grid(oskar_B200Workspace* ws, const oskar_B200Cube* cube,
+                    const oskar_B200Options* opt, size_t num_points,
+                    const void* uu, const void* vv, const void* ww,
+                    const void* vis, const void* weight, double cell_size_rad,
+                    double w_scale, int grid_size, void* grid,
+                    unsigned long long* d_num_skipped, double* d_norm,
+                    void* stream)
+{
+    if (!ws || !cube) return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    oskar_B200Options defaults;
+    oskar_b200_options_init(&defaults);
+    if (!opt) opt = &defaults;
+    int st = check_options(opt, cube->data_is_double);
+    if (st) return st;
+    st = check_grid_args(num_points, uu, vv, ww, vis, weight,
+                         opt->apply_weight, grid_size, grid);
+    if (st) return st;
+    if (cube->device != ws->device) return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    DeviceGuard g(ws->device);
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ws->stream;
+    return run_grid(ws, cube, opt, num_points, uu, vv, ww, vis, weight,
+                    cell_size_rad, w_scale, grid_size, grid, d_num_skipped,
+                    d_norm, s);
+}
+
+int oskar_b200_fold_compensation(oskar_B200Workspace* ws, void* grid,
+                                 int grid_size, void* stream)
+{
+    (void)ws; (void)grid; (void)grid_size; (void)stream;
+    return OSKAR_B200_ERR_UNSUPPORTED;
+}
+
+int oskar_b200_place(oskar_B200Workspace* ws, int data_is_double,
+                     int coord_mode, size_t num_w_planes, const int* support,
+                     int oversample, size_t num_points, const void* uu,
+                     const void* vv, const void* ww, double cell_size_rad,
+                     double w_scale, int grid_size, int32_t* gu, int32_t* gv,
+                     int32_t* plane, int32_t* off_u, int32_t* off_v,
+                     int32_t* conj, int32_t* skipped, void* stream)
+{
+    if (!ws || !support || num_w_planes == 0 || oversample < 1 ||
+        grid_size < 1 || (num_points && (!uu || !vv || !ww)))
+        return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    if (coord_mode != OSKAR_B200_COORDS_F64 &&
+        coord_mode != OSKAR_B200_COORDS_REFERENCE_F32)
+        return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    if (data_is_double && coord_mode != OSKAR_B200_COORDS_F64)
+        return OSKAR_B200_ERR_UNSUPPORTED;
+    DeviceGuard g(ws->device);
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ws->stream;
+    DeviceBuffer d_support;
+    cudaError_t e = d_support.ensure(sizeof(int) * num_w_planes);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_support.ptr, support, sizeof(int) * num_w_planes,
+                            cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return status_from_cuda(e);
+    int st = run_place(ws, data_is_double, coord_mode,
+                       static_cast<const int*>(d_support.ptr),
+                       (int)num_w_planes, oversample, num_points, uu, vv, ww,
+                       cell_size_rad, w_scale, grid_size, gu, gv, plane,
+                       off_u, off_v, conj, skipped, s);
+    e = cudaStreamSynchronize(s);  // d_support is freed on return
+    if (!st && e != cudaSuccess) st = status_from_cuda(e);
+    return st;
+}
+
+int oskar_b200_last_stats(oskar_B200Workspace* ws, oskar_B200Stats* stats)
+{
+    if (!ws || !stats) return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    const unsigned long long* c =
+        static_cast<const unsigned long long*>(ws->h_counters);
+    memset(stats, 0, sizeof(*stats));
+    stats->num_points = ws->last_points;
+    stats->num_gridded = ws->last_points - c[CNT_SKIPPED];
+    stats->grid_updates = c[CNT_UPDATES];
+    stats->num_tasks = c[CNT_TASKS];
+    stats->atomic_flushes = c[CNT_FLUSHES];
+    stats->status = c[CNT_STATUS] ? (c[CNT_STATUS] & DEV_ERR_TIMEOUT
+                                         ? OSKAR_B200_ERR_TIMEOUT
+                                         : OSKAR_B200_ERR_DEVICE_CHECK)
+                                  : OSKAR_B200_OK;
+    stats->kernel_launches = ws->last_launches;
+    if (ws->events_recorded)
+    {
+        DeviceGuard g(ws->device);
+        float* out[4] = {&stats->prep_ms, &stats->sort_ms, &stats->tasks_ms,
+                         &stats->grid_ms};
+        for (int i = 0; i < 4; ++i)
+            if (cudaEventElapsedTime(out[i], ws->events[i],
+                                     ws->events[i + 1]) != cudaSuccess)
+            {
+                cudaGetLastError();
+                *out[i] = 0.f;
+            }
+    }
+    return OSKAR_B200_OK;
+}
+
+int oskar_b200_set_stage_timing(oskar_B200Workspace* ws, int enable)
+{
+    if (!ws) return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    DeviceGuard g(ws->device);
+    if (enable)
+        for (cudaEvent_t& e : ws->events)
+            if (!e)
+            {
+                const cudaError_t r = cudaEventCreate(&e);
+                if (r != cudaSuccess) return status_from_cuda(r);
+            }
+    ws->stage_timing = enable ? 1 : 0;
+    ws->events_recorded = 0;
+    return OSKAR_B200_OK;
+}
+
+int oskar_b200_measure_atomic_rate(oskar_B200Workspace* ws, void* grid,
+                                   int grid_size, int iters,
+                                   double* updates_per_s)
+{
+    if (!ws || !grid || !updates_per_s) return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    DeviceGuard g(ws->device);
+    return measure_atomic_rate(ws, grid, grid_size, iters, updates_per_s);
+}
+
+const char* oskar_b200_build_info(void)
+{
+    return "fpga_gridding_b200 gridder; sm_100a; CUDA "
+#if defined(CUDART_VERSION)
+           B200_STR(CUDART_VERSION)
+#endif
+        ;
+}
+
+}  // extern "C"

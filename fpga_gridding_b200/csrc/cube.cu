@@ -1,0 +1,255 @@
+// Kernel-cube ingest: re-lays the reference's W-kernel cube into
+// phase-major per-plane slabs (see PlaneDesc in internal.h) in the storage
+// type the gridding kernel reads, and tabulates the per-(plane, offset) norm
+// contribution.
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+#include "internal.h"
+
+namespace b200 {
+namespace {
+
+template <typename KT> struct Store;
+template <> struct Store<float2>
+{
+    __device__ static float2 make(double re, double im, float inv)
+    {
+        return make_float2((float)re, (float)im);
+    }
+};
+template <> struct Store<double2>
+{
+    __device__ static double2 make(double re, double im, float inv)
+    {
+        return make_double2(re, im);
+    }
+};
+template <> struct Store<__half2>
+{
+    __device__ static __half2 make(double re, double im, float inv)
+    {
+        return __floats2half2_rn((float)re * inv, (float)im * inv);
+    }
+};
+template <> struct Store<__nv_bfloat162>
+{
+    __device__ static __nv_bfloat162 make(double re, double im, float inv)
+    {
+        return __floats2bfloat162_rn((float)re * inv, (float)im * inv);
+    }
+};
+
+// Largest |re| or |im| over each plane's used quadrant [0, E)^2, following
+// the reference's flat indexing (an index past the row end reads the next
+// row, as oskar_grid_wproj.c:110-116 does).
+template <typename IN>
+__global__ void plane_maxabs_kernel(const IN* __restrict__ cube,
+                                    const PlaneDesc* __restrict__ planes,
+                                    int conv_size_half, float* __restrict__ out)
+{
+    const int p = blockIdx.x;
+    const PlaneDesc d = planes[p];
+    const long long base = (long long)p * conv_size_half * conv_size_half;
+    float m = 0.f;
+    for (int e = threadIdx.x; e < d.extent * d.extent; e += blockDim.x)
+    {
+        const int xv = e / d.extent, xu = e % d.extent;
+        const long long f = base + (long long)xv * conv_size_half + xu;
+        m = fmaxf(m, fmaxf(fabsf((float)cube[2 * f]),
+                           fabsf((float)cube[2 * f + 1])));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    __shared__ float s_m[32];
+    if ((threadIdx.x & 31) == 0) s_m[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        float t = 0.f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t = fmaxf(t, s_m[w]);
+        out[p] = t;
+    }
+}
+
+template <typename IN, typename KT>
+__global__ void relayout_kernel(const IN* __restrict__ cube,
+                                const PlaneDesc* __restrict__ planes,
+                                int oversample, int conv_size_half,
+                                KT* __restrict__ slabs)
+{
+    const int p = blockIdx.y;
+    const PlaneDesc d = planes[p];
+    const long long base = (long long)p * conv_size_half * conv_size_half;
+    const int total = d.pitch * d.pitch;
+    const float inv = 1.0f / d.scale;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += gridDim.x * blockDim.x)
+    {
+        const int row = e / d.pitch, col = e % d.pitch;
+        // position = (x % os) * L + x / os  <=>  x = (pos % L) * os + pos / L
+        const int xv = (row % d.L) * oversample + row / d.L;
+        const int xu = (col % d.L) * oversample + col / d.L;
+        double re = 0.0, im = 0.0;
+        if (xv < d.extent && xu < d.extent && row / d.L < oversample &&
+            col / d.L < oversample)
+        {
+            const long long f = base + (long long)xv * conv_size_half + xu;
+            re = (double)cube[2 * f];
+            im = (double)cube[2 * f + 1];
+        }
+        slabs[d.offset + e] = Store<KT>::make(re, im, inv);
+    }
+}
+
+// Norm contribution of one visibility on plane p with offsets (off_u,
+// off_v): the real parts of its (2S+1)^2 taps summed in FP64 in the
+// reference's order (dv outer, du inner; oskar_grid_wproj.c:104-123), so a
+// per-visibility sum is bit-identical to the reference's `sum`.
+template <typename IN>
+__global__ void norm_table_kernel(const IN* __restrict__ cube,
+                                  const PlaneDesc* __restrict__ planes,
+                                  int num_planes, int oversample, int half,
+                                  int conv_size_half, double* __restrict__ table)
+{
+    const int span = 2 * half + 1;
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= num_planes * span * span) return;
+    const int p = idx / (span * span);
+    const int ov = (idx / span) % span - half;
+    const int ou = idx % span - half;
+    const int s = planes[p].support;
+    const long long base = (long long)p * conv_size_half * conv_size_half;
+    double acc = 0.0;
+    for (int dv = -s; dv <= s; ++dv)
+    {
+        const long long krow = base +
+            (long long)abs(ov + dv * oversample) * conv_size_half;
+        for (int du = -s; du <= s; ++du)
+            acc += (double)cube[2 * (krow + abs(ou + du * oversample))];
+    }
+    table[idx] = acc;
+}
+
+template <typename IN, typename KT>
+void launch_relayout(const oskar_B200Cube* c, const void* conv,
+                     cudaStream_t st)
+{
+    dim3 grid(64, c->num_planes);
+    relayout_kernel<IN, KT><<<grid, 256, 0, st>>>(
+        static_cast<const IN*>(conv),
+        static_cast<const PlaneDesc*>(c->d_planes.ptr), c->oversample,
+        c->conv_size_half, static_cast<KT*>(c->d_slabs.ptr));
+}
+
+}  // namespace
+
+int cube_build(oskar_B200Cube* c, const void* d_conv, int conv_is_double,
+               cudaStream_t st)
+{
+    const int P = c->num_planes, os = c->oversample;
+    // Slab geometry and offsets (host).
+    long long off = 0;
+    unsigned max_bytes = 0;
+    const size_t align_elems = 16 / c->elem_bytes > 0 ? 16 / c->elem_bytes : 1;
+    for (int p = 0; p < P; ++p)
+    {
+        PlaneDesc& d = c->planes[p];
+        d.extent = os * d.support + c->half + 1;
+        d.L = (d.extent + os - 1) / os;
+        d.pitch = os * d.L;
+        d.offset = off;
+        const size_t elems = (size_t)d.pitch * d.pitch;
+        const size_t padded = (elems + align_elems - 1) / align_elems *
+                              align_elems;
+        d.bytes = (unsigned)(padded * c->elem_bytes);
+        d.scale = 1.0f;
+        off += (long long)padded;
+        if (d.bytes > max_bytes) max_bytes = d.bytes;
+    }
+    c->max_slab_bytes = max_bytes;
+    cudaError_t e = c->d_planes.ensure(sizeof(PlaneDesc) * P);
+    if (e == cudaSuccess) e = c->d_slabs.ensure((size_t)off * c->elem_bytes);
+    if (e == cudaSuccess)
+        e = c->d_norm_table.ensure(sizeof(double) * P * (2 * c->half + 1) *
+                                   (2 * c->half + 1));
+    if (e != cudaSuccess) return status_from_cuda(e);
+
+    const bool scaled = c->kernel_type != OSKAR_B200_KERNEL_NATIVE;
+    if (scaled)
+    {
+        // Per-plane scale so the reduced-precision values use their full
+        // range: stored = value / max|value|.
+        e = cudaMemcpyAsync(c->d_planes.ptr, c->planes.data(),
+                            sizeof(PlaneDesc) * P, cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return status_from_cuda(e);
+        DeviceBuffer d_max;
+        e = d_max.ensure(sizeof(float) * P);
+        if (e != cudaSuccess) return status_from_cuda(e);
+        if (conv_is_double)
+            plane_maxabs_kernel<double><<<P, 256, 0, st>>>(
+                static_cast<const double*>(d_conv),
+                static_cast<const PlaneDesc*>(c->d_planes.ptr),
+                c->conv_size_half, static_cast<float*>(d_max.ptr));
+        else
+            plane_maxabs_kernel<float><<<P, 256, 0, st>>>(
+                static_cast<const float*>(d_conv),
+                static_cast<const PlaneDesc*>(c->d_planes.ptr),
+                c->conv_size_half, static_cast<float*>(d_max.ptr));
+        std::vector<float> h_max(P);
+        e = cudaMemcpyAsync(h_max.data(), d_max.ptr, sizeof(float) * P,
+                            cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return status_from_cuda(e);
+        for (int p = 0; p < P; ++p)
+            c->planes[p].scale = h_max[p] > 0.f ? h_max[p] : 1.0f;
+    }
+    e = cudaMemcpyAsync(c->d_planes.ptr, c->planes.data(),
+                        sizeof(PlaneDesc) * P, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return status_from_cuda(e);
+
+    if (conv_is_double)
+    {
+        switch (c->kernel_type)
+        {
+        case OSKAR_B200_KERNEL_F16:
+            launch_relayout<double, __half2>(c, d_conv, st); break;
+        case OSKAR_B200_KERNEL_BF16:
+            launch_relayout<double, __nv_bfloat162>(c, d_conv, st); break;
+        default:
+            if (c->data_is_double) launch_relayout<double, double2>(c, d_conv, st);
+            else launch_relayout<double, float2>(c, d_conv, st);
+        }
+    }
+    else
+    {
+        switch (c->kernel_type)
+        {
+        case OSKAR_B200_KERNEL_F16:
+            launch_relayout<float, __half2>(c, d_conv, st); break;
+        case OSKAR_B200_KERNEL_BF16:
+            launch_relayout<float, __nv_bfloat162>(c, d_conv, st); break;
+        default:
+            if (c->data_is_double) launch_relayout<float, double2>(c, d_conv, st);
+            else launch_relayout<float, float2>(c, d_conv, st);
+        }
+    }
+    const int span = 2 * c->half + 1;
+    const int entries = P * span * span;
+    const int blocks = (entries + 127) / 128;
+    if (conv_is_double)
+        norm_table_kernel<double><<<blocks, 128, 0, st>>>(
+            static_cast<const double*>(d_conv),
+            static_cast<const PlaneDesc*>(c->d_planes.ptr), P, os, c->half,
+            c->conv_size_half, static_cast<double*>(c->d_norm_table.ptr));
+    else
+        norm_table_kernel<float><<<blocks, 128, 0, st>>>(
+            static_cast<const float*>(d_conv),
+            static_cast<const PlaneDesc*>(c->d_planes.ptr), P, os, c->half,
+            c->conv_size_half, static_cast<double*>(c->d_norm_table.ptr));
+    return status_from_cuda(cudaGetLastError());
+}
+
+}  // namespace b200

@@ -1,0 +1,167 @@
+// Internal host-side declarations of the B200 gridder.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "oskar_grid_wproj_b200.h"
+
+namespace b200 {
+
+// ---------------------------------------------------------------------------
+// Re-laid kernel cube.
+//
+// The reference stores, per w-plane, the non-negative quadrant of the
+// oversampled kernel, indexed by |off + tap * oversample| in each axis
+// (oskar_grid_wproj.c:110-117).  A tap sequence tap = -S..S therefore walks
+// the quadrant with stride `oversample`.  Each plane is re-laid
+// "phase-major": quadrant index x goes to position (x % os) * L + x / os,
+// L = ceil(E / os), E = os * S + ceil(os / 2) + 1 (the entries the plane can
+// use).  Consecutive taps then read consecutive positions (one run for the
+// taps with off + tap * os >= 0 and one descending run for the rest), so a
+// warp's 32 kernel reads are contiguous in shared memory.
+// ---------------------------------------------------------------------------
+struct PlaneDesc
+{
+    int support;        // S
+    int extent;         // E
+    int L;              // positions per oversample phase
+    int pitch;          // row length of the slab in elements (os * L)
+    long long offset;   // element offset of the slab in the slab array
+    unsigned bytes;     // slab bytes, rounded up to 16
+    float scale;        // stored value = true value / scale (1 unless F16/BF16)
+};
+
+struct DeviceBuffer
+{
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    cudaError_t ensure(size_t n);  // grow-only; contents not preserved
+    void release();
+    ~DeviceBuffer();
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+};
+
+// Grid-launch tuning for one support size (the "autotuner" table entry).
+struct TuneEntry
+{
+    unsigned char classes_per_thread;  // 1, 2 or 4
+};
+
+}  // namespace b200
+
+// Opaque public types.
+struct oskar_B200Workspace
+{
+    int device = 0;
+    int num_sms = 0;
+    size_t smem_optin = 0;
+    cudaStream_t stream = nullptr;
+    // per-visibility work arrays
+    b200::DeviceBuffer keys[2], vals[2], rec, srec, svis, scan_tmp, flags;
+    b200::DeviceBuffer task_start;
+    // small arrays: counters, partial sums, plane histogram
+    b200::DeviceBuffer counters, partials, plane_counts;
+    // drop-in staging of the caller's host arrays
+    b200::DeviceBuffer in_uu, in_vv, in_ww, in_vis, in_weight, in_grid,
+        in_cube, in_norm;
+    // compensation grid of ACCUM_COMPENSATED
+    b200::DeviceBuffer comp_grid;
+    size_t comp_cells = 0;
+    // pinned host mirror of the device counters (stats)
+    void* h_counters = nullptr;
+    unsigned long long last_points = 0;
+    int last_launches = 0;
+    // stage timing (oskar_b200_set_stage_timing)
+    int stage_timing = 0;
+    int events_recorded = 0;
+    cudaEvent_t events[5] = {};
+};
+
+struct oskar_B200Cube
+{
+    int device = 0;
+    int num_planes = 0;
+    int oversample = 0;
+    int half = 0;            // ceil(oversample / 2): offsets lie in [-half, half]
+    int conv_size_half = 0;
+    int data_is_double = 0;
+    int kernel_type = OSKAR_B200_KERNEL_NATIVE;
+    int elem_bytes = 0;      // bytes per stored complex value
+    unsigned max_slab_bytes = 0;
+    int max_support = 0;
+    std::vector<b200::PlaneDesc> planes;
+    b200::DeviceBuffer d_planes, d_slabs, d_norm_table, d_support;
+};
+
+namespace b200 {
+
+// Counter slots in oskar_B200Workspace::counters (unsigned long long each).
+enum CounterSlot
+{
+    CNT_SKIPPED = 0,
+    CNT_TASKS = 1,
+    CNT_TASK_NEXT = 2,   // work-queue head of the gridding kernel
+    CNT_FLUSHES = 3,
+    CNT_STATUS = 4,      // DEV_ERR_* bits
+    CNT_UPDATES = 5,     // grid updates (taps) of gridded points
+    CNT_COUNT = 8
+};
+
+// ---- radix_sort.cu --------------------------------------------------------
+size_t scan_temp_bytes(size_t n);
+// Exclusive prefix sum of n uint32 values (out must not alias in).
+cudaError_t exclusive_scan_u32(const uint32_t* in, uint32_t* out, size_t n,
+                               void* temp, cudaStream_t st, int* launches);
+size_t radix_sort_temp_bytes(size_t n);
+// Stable LSD sort of (key, value) pairs on the low num_bits of the keys.
+// The sorted pairs end in keys[*which] / vals[*which].
+cudaError_t radix_sort_pairs(uint32_t* keys[2], uint32_t* vals[2], size_t n,
+                             int num_bits, void* temp, cudaStream_t st,
+                             int* which, int* launches);
+
+// ---- cube.cu ----------------------------------------------------------------
+int cube_build(oskar_B200Cube* cube, const void* d_conv_func,
+               int conv_func_is_double, cudaStream_t st);
+
+// ---- prep.cu / grid_romein.cu ---------------------------------------------
+struct KeyLayout
+{
+    int coarse_shift;  // log2 of the coarse tile side (cells)
+    int coarse_bits;   // bits per axis of the coarse tile index
+    int fine_shift;    // cells dropped inside a coarse tile
+    int fine_bits;     // bits per axis of the fine index
+    int plane_bits;
+    int total_bits;    // key bits below the skip flag
+};
+KeyLayout make_key_layout(int grid_size, int num_planes);
+
+int run_grid(oskar_B200Workspace* ws, const oskar_B200Cube* cube,
+             const oskar_B200Options* opt, size_t num_points, const void* uu,
+             const void* vv, const void* ww, const void* vis,
+             const void* weight, double cell_size_rad, double w_scale,
+             int grid_size, void* grid, unsigned long long* d_num_skipped,
+             double* d_norm, cudaStream_t st);
+
+int run_place(oskar_B200Workspace* ws, int data_is_double, int coord_mode,
+              const int* d_support, int num_planes, int oversample,
+              size_t num_points, const void* uu, const void* vv,
+              const void* ww, double cell_size_rad, double w_scale,
+              int grid_size, int32_t* gu, int32_t* gv, int32_t* plane,
+              int32_t* off_u, int32_t* off_v, int32_t* conj,
+              int32_t* skipped, cudaStream_t st);
+
+int fold_compensation(oskar_B200Workspace* ws, void* grid, int grid_size,
+                      cudaStream_t st);
+
+int measure_atomic_rate(oskar_B200Workspace* ws, void* grid, int grid_size,
+                        int iters, double* updates_per_s);
+
+int status_from_cuda(cudaError_t e);
+
+}  // namespace b200

@@ -1,0 +1,391 @@
+// Per-visibility preparation: placement (grid cell, w-plane, oversample
+// offsets, conjugation, skip test) exactly as oskar_grid_wproj.c:70-101
+// computes it, the sort key, the skip count, the norm, the plane histogram;
+// then, after the sort, the permutation into sorted order and the gridding
+// work list (tasks).
+#include "common.cuh"
+#include "internal.h"
+#include "prep.cuh"
+
+namespace b200 {
+
+KeyLayout make_key_layout(int grid_size, int num_planes)
+{
+    KeyLayout k{};
+    int gbits = 0;
+    while ((1 << gbits) < grid_size) ++gbits;
+    // Coarse tiles: at most 16 per axis and at least 64 cells wide, so the
+    // visibilities in flight at any time touch a few coarse tiles of grid.
+    k.coarse_shift = gbits - 4 > 6 ? gbits - 4 : 6;
+    int ctiles = (grid_size + (1 << k.coarse_shift) - 1) >> k.coarse_shift;
+    k.coarse_bits = 0;
+    while ((1 << k.coarse_bits) < ctiles) ++k.coarse_bits;
+    k.plane_bits = 0;
+    while ((1 << k.plane_bits) < num_planes) ++k.plane_bits;
+    k.fine_shift = 0;
+    k.fine_bits = k.coarse_shift;
+    while (2 * k.coarse_bits + k.plane_bits + 2 * k.fine_bits + 1 > 32 &&
+           k.fine_bits > 0)
+    {
+        ++k.fine_shift;
+        --k.fine_bits;
+    }
+    k.total_bits = 2 * k.coarse_bits + k.plane_bits + 2 * k.fine_bits;
+    return k;
+}
+
+namespace {
+
+constexpr int kPrepThreads = 256;
+constexpr int kMaxSmemPlanes = 4096;
+
+// Spreads the low 16 bits of x to the even bit positions.
+__device__ __forceinline__ uint32_t spread_bits(uint32_t x)
+{
+    x &= 0xffffu;
+    x = (x | (x << 8)) & 0x00ff00ffu;
+    x = (x | (x << 4)) & 0x0f0f0f0fu;
+    x = (x | (x << 2)) & 0x33333333u;
+    x = (x | (x << 1)) & 0x55555555u;
+    return x;
+}
+
+__device__ __forceinline__ uint32_t make_key(const KeyLayout& k, int gu,
+                                             int gv, int plane)
+{
+    const uint32_t cu = (uint32_t)gu >> k.coarse_shift;
+    const uint32_t cv = (uint32_t)gv >> k.coarse_shift;
+    const uint32_t in_mask = (1u << k.coarse_shift) - 1u;
+    const uint32_t fu = ((uint32_t)gu & in_mask) >> k.fine_shift;
+    const uint32_t fv = ((uint32_t)gv & in_mask) >> k.fine_shift;
+    const uint32_t coarse = spread_bits(cu) | (spread_bits(cv) << 1);
+    const uint32_t fine = spread_bits(fu) | (spread_bits(fv) << 1);
+    return (coarse << (k.plane_bits + 2 * k.fine_bits)) |
+           ((uint32_t)plane << (2 * k.fine_bits)) | fine;
+}
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(kPrepThreads)
+prep_kernel(const PrepArgs a)
+{
+    const T* __restrict__ uu = static_cast<const T*>(a.uu);
+    const T* __restrict__ vv = static_cast<const T*>(a.vv);
+    const T* __restrict__ ww = static_cast<const T*>(a.ww);
+    const T* __restrict__ wt = static_cast<const T*>(a.weight);
+    __shared__ unsigned s_hist[kMaxSmemPlanes];
+    __shared__ double s_norm[kPrepThreads / 32];
+    __shared__ unsigned s_skip[kPrepThreads / 32];
+    const bool smem_hist = a.num_planes <= kMaxSmemPlanes;
+    if (smem_hist)
+        for (int p = threadIdx.x; p < a.num_planes; p += blockDim.x)
+            s_hist[p] = 0;
+    __syncthreads();
+
+    const int span = 2 * a.half + 1;
+    const uint32_t skip_key = 1u << a.key.total_bits;
+    const int lane = threadIdx.x & 31;
+    double norm = 0.0;
+    unsigned skipped = 0;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t base = (size_t)blockIdx.x * blockDim.x; base < a.n;
+         base += stride)
+    {
+        const size_t i = base + threadIdx.x;
+        const bool in_range = i < a.n;
+        Placed p{};
+        if (in_range)
+            p = place_one<T, MODE>(uu[i], vv[i], ww[i], a.pc, a.support);
+        const bool keep = in_range && !p.skipped;
+        if (in_range)
+        {
+            if (keep)
+            {
+                a.rec[i] = make_int4(p.gu, p.gv,
+                                     p.plane | (p.conj < 0 ? (int)0x80000000 : 0),
+                                     (p.off_u + a.half) |
+                                         ((p.off_v + a.half) << 16));
+                a.keys[i] = make_key(a.key, p.gu, p.gv, p.plane);
+                double s = a.norm_table[((size_t)p.plane * span +
+                                         (p.off_v + a.half)) * span +
+                                        (p.off_u + a.half)];
+                if (a.apply_weight) s *= (double)wt[i];
+                norm += s;
+            }
+            else
+            {
+                a.keys[i] = skip_key;
+            }
+            a.vals[i] = (uint32_t)i;
+        }
+        skipped += in_range && !keep;
+        // plane histogram, aggregated across equal planes in the warp
+        const unsigned pl = keep ? (unsigned)p.plane : 0xffffffffu;
+        const unsigned peers = __match_any_sync(0xffffffffu, pl);
+        if (keep && lane == __ffs(peers) - 1)
+        {
+            if (smem_hist) atomicAdd(&s_hist[pl], (unsigned)__popc(peers));
+            else atomicAdd(&a.plane_counts[pl], (unsigned long long)__popc(peers));
+        }
+    }
+    norm = warp_sum(norm);
+    skipped = warp_sum(skipped);
+    if (lane == 0)
+    {
+        s_norm[threadIdx.x >> 5] = norm;
+        s_skip[threadIdx.x >> 5] = skipped;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        double t = 0.0;
+        unsigned long long k = 0;
+        for (int w = 0; w < kPrepThreads / 32; ++w)
+        {
+            t += s_norm[w];
+            k += s_skip[w];
+        }
+        a.norm_partials[blockIdx.x] = t;
+        if (k) atomicAdd(&a.counters[CNT_SKIPPED], k);
+    }
+    if (smem_hist)
+        for (int p = threadIdx.x; p < a.num_planes; p += blockDim.x)
+            if (s_hist[p])
+                atomicAdd(&a.plane_counts[p], (unsigned long long)s_hist[p]);
+}
+
+// Sums the per-block norm partials in a fixed order (deterministic), adds
+// them to the caller's norm, publishes the skip count, and counts grid
+// updates from the plane histogram.
+__global__ void finalize_prep_kernel(const double* __restrict__ partials,
+                                     int num_partials,
+                                     const unsigned long long* __restrict__ plane_counts,
+                                     const int* __restrict__ support,
+                                     int num_planes,
+                                     unsigned long long* __restrict__ counters,
+                                     double* __restrict__ d_norm,
+                                     unsigned long long* __restrict__ d_skipped)
+{
+    __shared__ double s_v[32];
+    __shared__ unsigned long long s_u[32];
+    double t = 0.0;
+    for (int i = threadIdx.x; i < num_partials; i += blockDim.x)
+        t += partials[i];
+    unsigned long long up = 0;
+    for (int p = threadIdx.x; p < num_planes; p += blockDim.x)
+    {
+        const unsigned long long w = 2ull * support[p] + 1ull;
+        up += plane_counts[p] * w * w;
+    }
+    t = warp_sum(t);
+    up = warp_sum(up);
+    if ((threadIdx.x & 31) == 0)
+    {
+        s_v[threadIdx.x >> 5] = t;
+        s_u[threadIdx.x >> 5] = up;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        double s = 0.0;
+        unsigned long long u = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
+        {
+            s += s_v[w];
+            u += s_u[w];
+        }
+        if (d_norm) *d_norm += s;
+        if (d_skipped) *d_skipped = counters[CNT_SKIPPED];
+        counters[CNT_UPDATES] = u;
+    }
+}
+
+template <typename T>
+__global__ void permute_kernel(const uint32_t* __restrict__ order, size_t n,
+                               const unsigned long long* __restrict__ counters,
+                               const int4* __restrict__ rec,
+                               const T* __restrict__ vis,
+                               const T* __restrict__ weight, int apply_weight,
+                               int4* __restrict__ srec, T* __restrict__ svis)
+{
+    const size_t valid = n - counters[CNT_SKIPPED];
+    for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < valid;
+         s += (size_t)gridDim.x * blockDim.x)
+    {
+        const uint32_t i = order[s];
+        srec[s] = rec[i];
+        T re = vis[2 * (size_t)i], im = vis[2 * (size_t)i + 1];
+        if (apply_weight)
+        {
+            const T w = weight[i];
+            re *= w;
+            im *= w;
+        }
+        svis[2 * s] = re;
+        svis[2 * s + 1] = im;
+    }
+}
+
+// Task boundaries: a new task starts where the (coarse tile, plane) part of
+// the sorted key changes, and every task_max positions.
+__global__ void task_flags_kernel(const uint32_t* __restrict__ keys, size_t n,
+                                  const unsigned long long* __restrict__ counters,
+                                  int fine_key_bits, int task_max,
+                                  uint32_t* __restrict__ flags)
+{
+    const size_t valid = n - counters[CNT_SKIPPED];
+    for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < n;
+         s += (size_t)gridDim.x * blockDim.x)
+    {
+        uint32_t f = 0;
+        if (s < valid)
+        {
+            f = (s == 0) || (s % (size_t)task_max == 0) ||
+                ((keys[s] >> fine_key_bits) != (keys[s - 1] >> fine_key_bits));
+        }
+        flags[s] = f;
+    }
+}
+
+__global__ void task_scatter_kernel(const uint32_t* __restrict__ flags,
+                                    const uint32_t* __restrict__ pos, size_t n,
+                                    unsigned long long* __restrict__ counters,
+                                    uint32_t* __restrict__ task_start)
+{
+    for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < n;
+         s += (size_t)gridDim.x * blockDim.x)
+    {
+        if (flags[s]) task_start[pos[s]] = (uint32_t)s;
+        if (s == n - 1)
+        {
+            const uint32_t num_tasks = pos[s] + flags[s];
+            counters[CNT_TASKS] = num_tasks;
+            task_start[num_tasks] = (uint32_t)(n - counters[CNT_SKIPPED]);
+        }
+    }
+}
+
+// Placement only, for inspection (oskar_b200_place).
+template <typename T, int MODE>
+__global__ void place_kernel(const T* __restrict__ uu, const T* __restrict__ vv,
+                             const T* __restrict__ ww, size_t n,
+                             PlaceConsts pc, const int* __restrict__ support,
+                             int32_t* gu, int32_t* gv, int32_t* plane,
+                             int32_t* off_u, int32_t* off_v, int32_t* conj,
+                             int32_t* skipped)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+    {
+        const Placed p = place_one<T, MODE>(uu[i], vv[i], ww[i], pc, support);
+        if (gu) gu[i] = p.gu_report;
+        if (gv) gv[i] = p.gv_report;
+        if (plane) plane[i] = p.plane;
+        if (off_u) off_u[i] = p.off_u;
+        if (off_v) off_v[i] = p.off_v;
+        if (conj) conj[i] = p.conj;
+        if (skipped) skipped[i] = p.skipped;
+    }
+}
+
+unsigned grid_blocks(size_t n, int num_sms, int per_sm, int threads)
+{
+    const size_t need = (n + threads - 1) / threads;
+    const size_t cap = (size_t)num_sms * per_sm;
+    return (unsigned)(need < cap ? (need > 0 ? need : 1) : cap);
+}
+
+}  // namespace
+
+unsigned prep_num_blocks(size_t n, int num_sms)
+{
+    return grid_blocks(n, num_sms, 8, kPrepThreads);
+}
+
+cudaError_t launch_prep(const PrepArgs& a, int data_is_double, int coord_mode,
+                        unsigned blocks, cudaStream_t st)
+{
+    if (data_is_double)
+        prep_kernel<double, COORD_F64><<<blocks, kPrepThreads, 0, st>>>(a);
+    else if (coord_mode == OSKAR_B200_COORDS_REFERENCE_F32)
+        prep_kernel<float, COORD_REF_F32><<<blocks, kPrepThreads, 0, st>>>(a);
+    else
+        prep_kernel<float, COORD_F64><<<blocks, kPrepThreads, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_finalize_prep(const double* partials, int num_partials,
+                                 const unsigned long long* plane_counts,
+                                 const int* support, int num_planes,
+                                 unsigned long long* counters, double* d_norm,
+                                 unsigned long long* d_skipped, cudaStream_t st)
+{
+    finalize_prep_kernel<<<1, 1024, 0, st>>>(partials, num_partials,
+                                             plane_counts, support, num_planes,
+                                             counters, d_norm, d_skipped);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_permute(const uint32_t* order, size_t n,
+                           const unsigned long long* counters, const int4* rec,
+                           const void* vis, const void* weight,
+                           int apply_weight, int data_is_double, int4* srec,
+                           void* svis, int num_sms, cudaStream_t st)
+{
+    const unsigned blocks = grid_blocks(n, num_sms, 8, 256);
+    if (data_is_double)
+        permute_kernel<double><<<blocks, 256, 0, st>>>(
+            order, n, counters, rec, static_cast<const double*>(vis),
+            static_cast<const double*>(weight), apply_weight, srec,
+            static_cast<double*>(svis));
+    else
+        permute_kernel<float><<<blocks, 256, 0, st>>>(
+            order, n, counters, rec, static_cast<const float*>(vis),
+            static_cast<const float*>(weight), apply_weight, srec,
+            static_cast<float*>(svis));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tasks(const uint32_t* sorted_keys, size_t n,
+                         unsigned long long* counters, int fine_key_bits,
+                         int task_max, uint32_t* flags, uint32_t* pos,
+                         void* scan_tmp, uint32_t* task_start, int num_sms,
+                         cudaStream_t st, int* launches)
+{
+    const unsigned blocks = grid_blocks(n, num_sms, 8, 256);
+    task_flags_kernel<<<blocks, 256, 0, st>>>(sorted_keys, n, counters,
+                                              fine_key_bits, task_max, flags);
+    cudaError_t e = exclusive_scan_u32(flags, pos, n, scan_tmp, st, launches);
+    if (e != cudaSuccess) return e;
+    if (launches) *launches += 2;
+    task_scatter_kernel<<<blocks, 256, 0, st>>>(flags, pos, n, counters,
+                                                task_start);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_place(int data_is_double, int coord_mode, const void* uu,
+                         const void* vv, const void* ww, size_t n,
+                         const PlaceConsts& pc, const int* support,
+                         int32_t* gu, int32_t* gv, int32_t* plane,
+                         int32_t* off_u, int32_t* off_v, int32_t* conj,
+                         int32_t* skipped, int num_sms, cudaStream_t st)
+{
+    const unsigned blocks = grid_blocks(n, num_sms, 8, 256);
+    if (data_is_double)
+        place_kernel<double, COORD_F64><<<blocks, 256, 0, st>>>(
+            static_cast<const double*>(uu), static_cast<const double*>(vv),
+            static_cast<const double*>(ww), n, pc, support, gu, gv, plane,
+            off_u, off_v, conj, skipped);
+    else if (coord_mode == OSKAR_B200_COORDS_REFERENCE_F32)
+        place_kernel<float, COORD_REF_F32><<<blocks, 256, 0, st>>>(
+            static_cast<const float*>(uu), static_cast<const float*>(vv),
+            static_cast<const float*>(ww), n, pc, support, gu, gv, plane,
+            off_u, off_v, conj, skipped);
+    else
+        place_kernel<float, COORD_F64><<<blocks, 256, 0, st>>>(
+            static_cast<const float*>(uu), static_cast<const float*>(vv),
+            static_cast<const float*>(ww), n, pc, support, gu, gv, plane,
+            off_u, off_v, conj, skipped);
+    return cudaGetLastError();
+}
+
+}  // namespace b200

@@ -1,0 +1,151 @@
+// Placement of one visibility and the prep launch interface.
+#pragma once
+
+#include <climits>
+
+#include "common.cuh"
+#include "internal.h"
+
+namespace b200 {
+
+enum { COORD_F64 = 0, COORD_REF_F32 = 1 };
+
+struct PlaceConsts
+{
+    double grid_scale;    // grid_size * cell_size_rad in FP64
+    double w_scale;
+    float grid_scale_f;   // grid_size * cell_size_rad rounded as in float C
+    float w_scale_f;
+    int grid_size;
+    int centre;           // grid_size / 2
+    int num_planes;
+    int oversample;
+};
+
+struct Placed
+{
+    int gu, gv;                 // valid when !skipped
+    int gu_report, gv_report;   // saturated to int32 for inspection
+    int plane;                  // clamped to the last plane
+    int off_u, off_v;
+    int conj;                   // -1 when w > 0, else +1
+    int skipped;
+};
+
+__device__ __forceinline__ int sat_i32(long long x)
+{
+    return x > INT_MAX ? INT_MAX : (x < INT_MIN ? INT_MIN : (int)x);
+}
+
+// oskar_grid_wproj.c:70-101 (FP64) or :168-212 (float, MODE ==
+// COORD_REF_F32).  Every rounding step is an explicit IEEE operation so
+// the result is bit-identical to the C code on the same inputs:
+//   pos = -u * grid_scale, v * grid_scale
+//   grid_w = round(sqrt(|w * w_scale|)), clamped to the last plane
+//   grid_u = (int)round(pos_u) + grid_size / 2     (same for v)
+//   off_u = (int)round((round(pos_u) - pos_u) * oversample)
+//   skipped when grid_u +- S or grid_v +- S leaves [0, grid_size).
+// round() is half-away-from-zero on both sides.  A coordinate whose rounded
+// value is outside the int range (or NaN) is placed at INT_MIN, as x86-64's
+// truncating conversion does, and is therefore skipped.
+template <typename T, int MODE>
+__device__ __forceinline__ Placed place_one(T u, T v, T w,
+                                            const PlaceConsts& c,
+                                            const int* __restrict__ support)
+{
+    Placed p;
+    long long gu, gv;
+    if (MODE == COORD_F64)
+    {
+        const double du = (double)u, dv = (double)v, dw = (double)w;
+        const double pos_u = __dmul_rn(-du, c.grid_scale);
+        const double pos_v = __dmul_rn(dv, c.grid_scale);
+        p.conj = dw > 0.0 ? -1 : 1;
+        const double wr = round(sqrt(fabs(__dmul_rn(dw, c.w_scale))));
+        p.plane = wr < (double)c.num_planes ? (int)wr : c.num_planes - 1;
+        const double ru = round(pos_u), rv = round(pos_v);
+        const bool oku = ru > -2147483649.0 && ru < 2147483648.0;
+        const bool okv = rv > -2147483649.0 && rv < 2147483648.0;
+        gu = (oku ? (long long)ru : (long long)INT_MIN) + c.centre;
+        gv = (okv ? (long long)rv : (long long)INT_MIN) + c.centre;
+        p.off_u = (int)round(__dmul_rn(__dsub_rn(ru, pos_u),
+                                       (double)c.oversample));
+        p.off_v = (int)round(__dmul_rn(__dsub_rn(rv, pos_v),
+                                       (double)c.oversample));
+    }
+    else
+    {
+        const float fu = (float)u, fv = (float)v, fw = (float)w;
+        const float pos_u = __fmul_rn(-fu, c.grid_scale_f);
+        const float pos_v = __fmul_rn(fv, c.grid_scale_f);
+        p.conj = fw > 0.0f ? -1 : 1;
+        const float wr = roundf(sqrtf(fabsf(__fmul_rn(fw, c.w_scale_f))));
+        p.plane = wr < (float)c.num_planes ? (int)wr : c.num_planes - 1;
+        const float ru = roundf(pos_u), rv = roundf(pos_v);
+        const bool oku = ru > -2147483649.0f && ru < 2147483648.0f;
+        const bool okv = rv > -2147483649.0f && rv < 2147483648.0f;
+        gu = (oku ? (long long)ru : (long long)INT_MIN) + c.centre;
+        gv = (okv ? (long long)rv : (long long)INT_MIN) + c.centre;
+        p.off_u = (int)roundf(__fmul_rn(__fsub_rn(ru, pos_u),
+                                        (float)c.oversample));
+        p.off_v = (int)roundf(__fmul_rn(__fsub_rn(rv, pos_v),
+                                        (float)c.oversample));
+    }
+    const int s = support[p.plane];
+    p.skipped = (gu + s >= c.grid_size) || (gu - s < 0) ||
+                (gv + s >= c.grid_size) || (gv - s < 0);
+    p.gu = (int)gu;
+    p.gv = (int)gv;
+    p.gu_report = sat_i32(gu);
+    p.gv_report = sat_i32(gv);
+    return p;
+}
+
+struct PrepArgs
+{
+    const void* uu;
+    const void* vv;
+    const void* ww;
+    const void* weight;
+    size_t n;
+    PlaceConsts pc;
+    const int* support;
+    int num_planes;
+    int half;
+    int apply_weight;
+    const double* norm_table;
+    KeyLayout key;
+    int4* rec;
+    uint32_t* keys;
+    uint32_t* vals;
+    unsigned long long* counters;
+    double* norm_partials;
+    unsigned long long* plane_counts;
+};
+
+unsigned prep_num_blocks(size_t n, int num_sms);
+cudaError_t launch_prep(const PrepArgs& a, int data_is_double, int coord_mode,
+                        unsigned blocks, cudaStream_t st);
+cudaError_t launch_finalize_prep(const double* partials, int num_partials,
+                                 const unsigned long long* plane_counts,
+                                 const int* support, int num_planes,
+                                 unsigned long long* counters, double* d_norm,
+                                 unsigned long long* d_skipped, cudaStream_t st);
+cudaError_t launch_permute(const uint32_t* order, size_t n,
+                           const unsigned long long* counters, const int4* rec,
+                           const void* vis, const void* weight,
+                           int apply_weight, int data_is_double, int4* srec,
+                           void* svis, int num_sms, cudaStream_t st);
+cudaError_t launch_tasks(const uint32_t* sorted_keys, size_t n,
+                         unsigned long long* counters, int fine_key_bits,
+                         int task_max, uint32_t* flags, uint32_t* pos,
+                         void* scan_tmp, uint32_t* task_start, int num_sms,
+                         cudaStream_t st, int* launches);
+cudaError_t launch_place(int data_is_double, int coord_mode, const void* uu,
+                         const void* vv, const void* ww, size_t n,
+                         const PlaceConsts& pc, const int* support,
+                         int32_t* gu, int32_t* gv, int32_t* plane,
+                         int32_t* off_u, int32_t* off_v, int32_t* conj,
+                         int32_t* skipped, int num_sms, cudaStream_t st);
+
+}  // namespace b200

@@ -1,0 +1,295 @@
+// Device prefix sum and stable LSD radix sort of (uint32 key, uint32 value)
+// pairs, written for this project (no CUB).
+//
+// Radix sort: 8-bit digits, one pass per digit.  Each pass is
+//   1. rs_histogram: per 4096-key tile, per-digit counts, stored digit-major
+//      (counts[digit * num_tiles + tile]);
+//   2. exclusive scan of that array: the output position of the first key of
+//      each (digit, tile);
+//   3. rs_scatter: stable ranks inside the tile, scatter to the output.
+// Inside a tile each warp owns a contiguous run of 512 keys, read as 16
+// coalesced 32-key rows.  Equal digits in a row are ranked with
+// __match_any_sync against warp-private running counts, so the whole tile
+// needs only two block barriers.
+#include "common.cuh"
+#include "internal.h"
+
+namespace b200 {
+namespace {
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;  // 2048
+
+constexpr int kSortThreads = 256;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 4096
+constexpr int kRadix = 256;
+
+// ---------------------------------------------------------------------------
+// Scan
+// ---------------------------------------------------------------------------
+
+// Block-wide exclusive scan of one value per thread; returns the block total.
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v,
+                                                         uint32_t* s_warp,
+                                                         uint32_t* total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1)
+    {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += t;
+    }
+    if (lane == 31) s_warp[warp] = inc;
+    __syncthreads();
+    if (warp == 0)
+    {
+        uint32_t w = lane < (int)(blockDim.x >> 5) ? s_warp[lane] : 0;
+        uint32_t wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += t;
+        }
+        if (lane < (int)(blockDim.x >> 5)) s_warp[lane] = wi - w;
+        if (lane == 31) *total = wi;
+    }
+    __syncthreads();
+    return s_warp[warp] + inc - v;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+scan_reduce_kernel(const uint32_t* __restrict__ in, size_t n,
+                   uint32_t* __restrict__ block_sums)
+{
+    const size_t base = (size_t)blockIdx.x * kScanTile;
+    uint32_t s = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i)
+    {
+        const size_t p = base + (size_t)i * kScanThreads + threadIdx.x;
+        if (p < n) s += in[p];
+    }
+    s = warp_sum(s);
+    __shared__ uint32_t s_w[kScanThreads / 32];
+    if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        uint32_t t = 0;
+        for (int w = 0; w < kScanThreads / 32; ++w) t += s_w[w];
+        block_sums[blockIdx.x] = t;
+    }
+}
+
+// One block scans the block sums in place (exclusive).
+__global__ void __launch_bounds__(1024)
+scan_block_sums_kernel(uint32_t* __restrict__ sums, size_t count)
+{
+    __shared__ uint32_t s_warp[32];
+    __shared__ uint32_t s_total;
+    uint32_t carry = 0;
+    for (size_t base = 0; base < count; base += blockDim.x)
+    {
+        const size_t p = base + threadIdx.x;
+        const uint32_t v = p < count ? sums[p] : 0;
+        const uint32_t ex = block_exclusive_scan(v, s_warp, &s_total);
+        if (p < count) sums[p] = carry + ex;
+        carry += s_total;
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+scan_apply_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
+                  size_t n, const uint32_t* __restrict__ block_offsets)
+{
+    __shared__ uint32_t s_warp[32];
+    __shared__ uint32_t s_total;
+    // Thread t scans items [t * 8, t * 8 + 8) of the tile.
+    const size_t base = (size_t)blockIdx.x * kScanTile +
+                        (size_t)threadIdx.x * kScanItems;
+    uint32_t v[kScanItems];
+    uint32_t s = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i)
+    {
+        v[i] = (base + i < n) ? in[base + i] : 0;
+        s += v[i];
+    }
+    uint32_t run = block_exclusive_scan(s, s_warp, &s_total) +
+                   block_offsets[blockIdx.x];
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i)
+    {
+        if (base + i < n) out[base + i] = run;
+        run += v[i];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Radix sort passes
+// ---------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(kSortThreads)
+rs_histogram_kernel(const uint32_t* __restrict__ keys, size_t n, int shift,
+                    uint32_t mask, size_t num_tiles,
+                    uint32_t* __restrict__ counts)
+{
+    __shared__ uint32_t s_count[kSortWarps][kRadix];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < kSortWarps * kRadix; i += kSortThreads)
+        (&s_count[0][0])[i] = 0;
+    __syncthreads();
+    const size_t base = (size_t)blockIdx.x * kSortTile +
+                        (size_t)warp * (32 * kSortItems);
+#pragma unroll 4
+    for (int i = 0; i < kSortItems; ++i)
+    {
+        const size_t p = base + (size_t)i * 32 + lane;
+        const unsigned d = p < n ? ((keys[p] >> shift) & mask) : kRadix;
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        if (d < kRadix && lane == __ffs(peers) - 1)
+            s_count[warp][d] += __popc(peers);
+    }
+    __syncthreads();
+    for (int d = threadIdx.x; d < kRadix; d += kSortThreads)
+    {
+        uint32_t t = 0;
+#pragma unroll
+        for (int w = 0; w < kSortWarps; ++w) t += s_count[w][d];
+        counts[(size_t)d * num_tiles + blockIdx.x] = t;
+    }
+}
+
+__global__ void __launch_bounds__(kSortThreads)
+rs_scatter_kernel(const uint32_t* __restrict__ keys_in,
+                  const uint32_t* __restrict__ vals_in, size_t n, int shift,
+                  uint32_t mask, size_t num_tiles,
+                  const uint32_t* __restrict__ offsets,
+                  uint32_t* __restrict__ keys_out,
+                  uint32_t* __restrict__ vals_out)
+{
+    __shared__ uint32_t s_count[kSortWarps][kRadix];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    for (int i = threadIdx.x; i < kSortWarps * kRadix; i += kSortThreads)
+        (&s_count[0][0])[i] = 0;
+    __syncthreads();
+
+    const size_t base = (size_t)blockIdx.x * kSortTile +
+                        (size_t)warp * (32 * kSortItems);
+    uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
+#pragma unroll
+    for (int i = 0; i < kSortItems; ++i)
+    {
+        const size_t p = base + (size_t)i * 32 + lane;
+        const bool ok = p < n;
+        key[i] = ok ? keys_in[p] : 0u;
+        val[i] = ok ? vals_in[p] : 0u;
+        const unsigned d = ok ? ((key[i] >> shift) & mask) : kRadix;
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        uint32_t before = 0;
+        if (d < kRadix) before = s_count[warp][d];
+        __syncwarp();
+        if (d < kRadix && lane == __ffs(peers) - 1)
+            s_count[warp][d] = before + __popc(peers);
+        __syncwarp();
+        rank[i] = before + __popc(peers & lt_mask);
+    }
+    __syncthreads();
+    // Turn the per-warp counts into output positions: warps in order, each
+    // digit starting at its scanned (digit, tile) offset.
+    for (int d = threadIdx.x; d < kRadix; d += kSortThreads)
+    {
+        uint32_t run = offsets[(size_t)d * num_tiles + blockIdx.x];
+#pragma unroll
+        for (int w = 0; w < kSortWarps; ++w)
+        {
+            const uint32_t c = s_count[w][d];
+            s_count[w][d] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < kSortItems; ++i)
+    {
+        const size_t p = base + (size_t)i * 32 + lane;
+        if (p < n)
+        {
+            const unsigned d = (key[i] >> shift) & mask;
+            const uint32_t dst = s_count[warp][d] + rank[i];
+            keys_out[dst] = key[i];
+            vals_out[dst] = val[i];
+        }
+    }
+}
+
+size_t scan_blocks(size_t n) { return (n + kScanTile - 1) / kScanTile; }
+
+}  // namespace
+
+size_t scan_temp_bytes(size_t n)
+{
+    return (scan_blocks(n) + 1) * sizeof(uint32_t);
+}
+
+cudaError_t exclusive_scan_u32(const uint32_t* in, uint32_t* out, size_t n,
+                               void* temp, cudaStream_t st, int* launches)
+{
+    if (n == 0) return cudaSuccess;
+    if (launches) *launches += 3;
+    const size_t nb = scan_blocks(n);
+    uint32_t* sums = static_cast<uint32_t*>(temp);
+    scan_reduce_kernel<<<(unsigned)nb, kScanThreads, 0, st>>>(in, n, sums);
+    scan_block_sums_kernel<<<1, 1024, 0, st>>>(sums, nb);
+    scan_apply_kernel<<<(unsigned)nb, kScanThreads, 0, st>>>(in, out, n, sums);
+    return cudaGetLastError();
+}
+
+size_t radix_sort_temp_bytes(size_t n)
+{
+    const size_t tiles = (n + kSortTile - 1) / kSortTile;
+    const size_t counts = tiles * kRadix;
+    // counts + scanned offsets + scan scratch
+    return 2 * counts * sizeof(uint32_t) + scan_temp_bytes(counts) + 256;
+}
+
+cudaError_t radix_sort_pairs(uint32_t* keys[2], uint32_t* vals[2], size_t n,
+                             int num_bits, void* temp, cudaStream_t st,
+                             int* which, int* launches)
+{
+    *which = 0;
+    if (n <= 1 || num_bits <= 0) return cudaSuccess;
+    const size_t tiles = (n + kSortTile - 1) / kSortTile;
+    const size_t ncount = tiles * kRadix;
+    uint32_t* counts = static_cast<uint32_t*>(temp);
+    uint32_t* offsets = counts + ncount;
+    void* scan_tmp = offsets + ncount;
+    int cur = 0;
+    for (int shift = 0; shift < num_bits; shift += 8)
+    {
+        const int bits = num_bits - shift < 8 ? num_bits - shift : 8;
+        const uint32_t mask = (1u << bits) - 1u;
+        rs_histogram_kernel<<<(unsigned)tiles, kSortThreads, 0, st>>>(
+            keys[cur], n, shift, mask, tiles, counts);
+        cudaError_t e = exclusive_scan_u32(counts, offsets, ncount, scan_tmp,
+                                           st, launches);
+        if (e != cudaSuccess) return e;
+        rs_scatter_kernel<<<(unsigned)tiles, kSortThreads, 0, st>>>(
+            keys[cur], vals[cur], n, shift, mask, tiles, offsets,
+            keys[cur ^ 1], vals[cur ^ 1]);
+        if (launches) *launches += 2;
+        cur ^= 1;
+    }
+    *which = cur;
+    return cudaGetLastError();
+}
+
+}  // namespace b200

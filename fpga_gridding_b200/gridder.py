@@ -1,0 +1,228 @@
+"""Python front end of the B200 gridder.
+
+`oskar_grid_wproj_d` / `oskar_grid_wproj_f` mirror the reference's C
+functions (oskar_grid_wproj.h:69-86, :114-131): same argument order and
+meaning, host (numpy) arrays, grid updated in place.  The C out-parameters
+num_skipped and norm come back as the return value (num_skipped, norm),
+norm being the updated accumulator.  Failures raise GridderError instead of
+the reference's silent behaviour.
+
+`Workspace`, `Cube`, `grid_device` and `place_device` wrap the extended,
+device-resident API for torch CUDA tensors.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import GridderError, Options, Stats, check, load
+
+
+def _carr(a, dtype):
+    a = np.asarray(a)
+    if a.dtype != dtype or not a.flags.c_contiguous:
+        raise TypeError(f"expected a C-contiguous {np.dtype(dtype).name} array")
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _dropin(fn, real, num_w_planes, support, oversample, conv_size_half,
+            conv_func, num_points, uu, vv, ww, vis, weight, cell_size_rad,
+            w_scale, grid_size, norm, grid):
+    lib = load()
+    support = np.ascontiguousarray(support, dtype=np.int32)
+    skipped = C.c_size_t(0)
+    nrm = C.c_double(norm)
+    args = [num_w_planes, _carr(support, np.int32), oversample,
+            conv_size_half, _carr(conv_func, real), num_points]
+    for a in (uu, vv, ww, vis):
+        args.append(_carr(a, real))
+    args.append(_carr(weight, real) if weight is not None else None)
+    args += [cell_size_rad, w_scale, grid_size, C.byref(skipped),
+             C.byref(nrm), _carr(grid, real)]
+    fn(*args)
+    check(lib.oskar_grid_wproj_b200_last_error(), fn.__name__)
+    return skipped.value, nrm.value
+
+
+def oskar_grid_wproj_d(num_w_planes, support, oversample, conv_size_half,
+                       conv_func, num_points, uu, vv, ww, vis, weight,
+                       cell_size_rad, w_scale, grid_size, norm, grid):
+    """FP64 drop-in.  Returns (num_skipped, norm); grid accumulates."""
+    return _dropin(load().oskar_grid_wproj_d, np.float64, num_w_planes,
+                   support, oversample, conv_size_half, conv_func,
+                   num_points, uu, vv, ww, vis, weight, cell_size_rad,
+                   w_scale, grid_size, norm, grid)
+
+
+def oskar_grid_wproj_f(num_w_planes, support, oversample, conv_size_half,
+                       conv_func, num_points, uu, vv, ww, vis, weight,
+                       cell_size_rad, w_scale, grid_size, norm, grid):
+    """FP32 drop-in (FP64 coordinates).  Returns (num_skipped, norm)."""
+    return _dropin(load().oskar_grid_wproj_f, np.float32, num_w_planes,
+                   support, oversample, conv_size_half, conv_func,
+                   num_points, uu, vv, ww, vis, weight, cell_size_rad,
+                   w_scale, grid_size, norm, grid)
+
+
+def grid_workload(w: dict, single: bool, grid=None, norm: float = 0.0):
+    """Drop-in call on a Workload.numpy() dict.  Returns
+    (num_skipped, norm, grid)."""
+    real = np.float32 if single else np.float64
+    g = w["grid_size"]
+    if grid is None:
+        grid = np.zeros(2 * g * g, dtype=real)
+    fn = oskar_grid_wproj_f if single else oskar_grid_wproj_d
+    conv = lambda k: np.ascontiguousarray(w[k], dtype=real)
+    sk, nrm = fn(w["num_w_planes"], w["support"], w["oversample"],
+                 w["conv_size_half"], conv("conv_func"), len(w["uu"]),
+                 conv("uu"), conv("vv"), conv("ww"), conv("vis"),
+                 conv("weight"), w["cell_size_rad"], w["w_scale"], g, norm,
+                 grid)
+    return sk, nrm, grid
+
+
+# --------------------------------------------------------------------------
+# Extended API (device-resident, torch tensors)
+# --------------------------------------------------------------------------
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        return None
+    return C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream")
+                      else int(stream))
+
+
+def options(**kw) -> Options:
+    o = Options()
+    load().oskar_b200_options_init(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+class Workspace:
+    """Device buffers and a default stream for one device."""
+
+    def __init__(self, device: int = 0):
+        self._lib = load()
+        self.handle = C.c_void_p()
+        check(self._lib.oskar_b200_workspace_create(device,
+                                                   C.byref(self.handle)),
+              "workspace_create")
+        self.device = device
+
+    def close(self):
+        if self.handle:
+            self._lib.oskar_b200_workspace_free(self.handle)
+            self.handle = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def bytes(self) -> int:
+        return int(self._lib.oskar_b200_workspace_bytes(self.handle))
+
+    def stats(self) -> Stats:
+        s = Stats()
+        check(self._lib.oskar_b200_last_stats(self.handle, C.byref(s)),
+              "last_stats")
+        return s
+
+
+class Cube:
+    """A W-kernel cube re-laid and resident on the device."""
+
+    def __init__(self, ws: Workspace, support, oversample: int,
+                 conv_size_half: int, conv_func, data_is_double: bool,
+                 kernel_type: int = _lib.KERNEL_NATIVE, stream=None):
+        import torch
+        self._lib = load()
+        self.support = np.ascontiguousarray(support, dtype=np.int32)
+        on_device = isinstance(conv_func, torch.Tensor) and conv_func.is_cuda
+        if isinstance(conv_func, torch.Tensor):
+            conv_func = conv_func.contiguous()
+            is_double = conv_func.dtype == torch.float64
+            ptr = C.c_void_p(conv_func.data_ptr())
+        else:
+            conv_func = np.ascontiguousarray(conv_func)
+            is_double = conv_func.dtype == np.float64
+            ptr = conv_func.ctypes.data_as(C.c_void_p)
+        self.handle = C.c_void_p()
+        check(self._lib.oskar_b200_cube_create(
+            ws.handle, len(self.support),
+            self.support.ctypes.data_as(C.c_void_p), oversample,
+            conv_size_half, ptr, int(is_double), int(on_device),
+            int(data_is_double), kernel_type, _stream_ptr(stream),
+            C.byref(self.handle)), "cube_create")
+        self.data_is_double = data_is_double
+        self.kernel_type = kernel_type
+
+    def close(self):
+        if self.handle:
+            self._lib.oskar_b200_cube_free(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def bytes(self) -> int:
+        return int(self._lib.oskar_b200_cube_bytes(self.handle))
+
+
+def grid_device(ws: Workspace, cube: Cube, uu, vv, ww, vis, weight,
+                cell_size_rad: float, w_scale: float, grid_size: int, grid,
+                d_num_skipped=None, d_norm=None, opts: Options | None = None,
+                stream=None) -> None:
+    """Asynchronous gridding of device tensors into `grid` (accumulates).
+    d_num_skipped (uint64/int64 device scalar) is overwritten, d_norm
+    (float64 device scalar) incremented."""
+    lib = load()
+    if opts is None:
+        opts = options()
+    n = uu.numel()
+    check(lib.oskar_b200_grid(
+        ws.handle, cube.handle, C.byref(opts), n, _ptr(uu), _ptr(vv),
+        _ptr(ww), _ptr(vis), _ptr(weight), float(cell_size_rad),
+        float(w_scale), grid_size, _ptr(grid), _ptr(d_num_skipped),
+        _ptr(d_norm), _stream_ptr(stream)), "oskar_b200_grid")
+
+
+def place_device(ws: Workspace, support, oversample: int, uu, vv, ww,
+                 cell_size_rad: float, w_scale: float, grid_size: int,
+                 coord_mode: int = _lib.COORDS_F64, stream=None) -> dict:
+    """Per-visibility placement as computed on the device (synchronous).
+    Returns int32 device tensors gu, gv, plane, off_u, off_v, conj, skipped."""
+    import torch
+    lib = load()
+    support = np.ascontiguousarray(support, dtype=np.int32)
+    n = uu.numel()
+    out = {k: torch.empty(n, dtype=torch.int32, device=uu.device)
+           for k in ("gu", "gv", "plane", "off_u", "off_v", "conj", "skipped")}
+    check(lib.oskar_b200_place(
+        ws.handle, int(uu.dtype == torch.float64), coord_mode, len(support),
+        support.ctypes.data_as(C.c_void_p), oversample, n, _ptr(uu),
+        _ptr(vv), _ptr(ww), float(cell_size_rad), float(w_scale), grid_size,
+        *[_ptr(out[k]) for k in ("gu", "gv", "plane", "off_u", "off_v",
+                                 "conj", "skipped")],
+        _stream_ptr(stream)), "oskar_b200_place")
+    return out

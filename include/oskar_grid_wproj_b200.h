@@ -1,0 +1,255 @@
+/*
+ * oskar_grid_wproj_b200.h -- B200 (sm_100a) W-projection gridder, C ABI.
+ *
+ * Library: fpga_gridding_b200/libgridder_b200.so
+ *
+ * 1. Drop-in entry points with exactly the reference's signatures
+ *    (oskar_grid_wproj.h:69-86 and :114-131 of OxfordSKA/FPGA_Gridding).
+ *    All pointers are host memory, the call is synchronous, num_skipped is
+ *    reset, norm and grid accumulate, weight is ignored (as the reference
+ *    hard-codes weight 1.0, oskar_grid_wproj.c:80-81).  Like the reference
+ *    they return void; a failure leaves grid/norm untouched and is readable
+ *    with oskar_grid_wproj_b200_last_error() from the same thread.
+ *
+ * 2. An extended, asynchronous API on device-resident buffers with explicit
+ *    stream, workspace, resident kernel cubes and precision options.  Every
+ *    extended function returns an oskar_B200Status.
+ *
+ * There is no CPU fallback: without a usable CUDA device every entry point
+ * fails with OSKAR_B200_ERR_NO_DEVICE.
+ */
+#ifndef OSKAR_GRID_WPROJ_B200_H_
+#define OSKAR_GRID_WPROJ_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define OSKAR_B200_EXPORT __attribute__((visibility("default")))
+#else
+#define OSKAR_B200_EXPORT
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------------- */
+/* Status codes                                                           */
+/* ---------------------------------------------------------------------- */
+typedef enum
+{
+    OSKAR_B200_OK = 0,
+    OSKAR_B200_ERR_INVALID_ARGUMENT = 1, /* sizes, null pointers, cube extent */
+    OSKAR_B200_ERR_NO_DEVICE = 2,        /* no usable CUDA device */
+    OSKAR_B200_ERR_OUT_OF_MEMORY = 3,    /* device or pinned host allocation */
+    OSKAR_B200_ERR_CUDA = 4,             /* any other CUDA runtime error */
+    OSKAR_B200_ERR_UNSUPPORTED = 5,      /* option combination not built */
+    OSKAR_B200_ERR_DEVICE_CHECK = 6,     /* a kernel's own bounds check fired */
+    OSKAR_B200_ERR_TIMEOUT = 7,          /* a bounded device-side wait expired */
+    OSKAR_B200_ERR_OVER_BUDGET = 8       /* job exceeds the HBM budget */
+} oskar_B200Status;
+
+/* ---------------------------------------------------------------------- */
+/* 1. Drop-in replacements                                                */
+/* ---------------------------------------------------------------------- */
+
+/* Replaces oskar_grid_wproj_d (oskar_grid_wproj.h:69-86).  FP64 data,
+ * FP64 grid, FP64 coordinates; grid within 1e-12 relative RMS of the
+ * reference, num_skipped and every placement bit-exact. */
+OSKAR_B200_EXPORT
+void oskar_grid_wproj_d(
+        const size_t num_w_planes,
+        const int* support,
+        const int oversample,
+        const int conv_size_half,
+        const double* conv_func,
+        const size_t num_points,
+        const double* uu,
+        const double* vv,
+        const double* ww,
+        const double* vis,
+        const double* weight,
+        const double cell_size_rad,
+        const double w_scale,
+        const int grid_size,
+        size_t* num_skipped,
+        double* norm,
+        double* grid);
+
+/* Replaces oskar_grid_wproj_f (oskar_grid_wproj.h:114-131).  FP32 data,
+ * kernel and grid; grid coordinates, w-plane and oversample offsets are
+ * computed in FP64 from the float inputs (so placements equal the FP64
+ * reference's on the same inputs); norm is FP64.  The reference's float
+ * coordinate arithmetic is available through the extended API
+ * (OSKAR_B200_COORDS_REFERENCE_F32). */
+OSKAR_B200_EXPORT
+void oskar_grid_wproj_f(
+        const size_t num_w_planes,
+        const int* support,
+        const int oversample,
+        const int conv_size_half,
+        const float* conv_func,
+        const size_t num_points,
+        const float* uu,
+        const float* vv,
+        const float* ww,
+        const float* vis,
+        const float* weight,
+        const float cell_size_rad,
+        const float w_scale,
+        const int grid_size,
+        size_t* num_skipped,
+        double* norm,
+        float* grid);
+
+/* Status of the calling thread's most recent drop-in call. */
+OSKAR_B200_EXPORT int oskar_grid_wproj_b200_last_error(void);
+
+/* Static description of a status code. */
+OSKAR_B200_EXPORT const char* oskar_grid_wproj_b200_error_string(int status);
+
+/* Frees the calling thread's cached device buffers and stream (the drop-ins
+ * keep them between calls to avoid re-allocation). */
+OSKAR_B200_EXPORT void oskar_grid_wproj_b200_release_thread_cache(void);
+
+/* ---------------------------------------------------------------------- */
+/* 2. Extended API                                                        */
+/* ---------------------------------------------------------------------- */
+
+/* Coordinate arithmetic for (grid_u, grid_v, w-plane, offsets). */
+enum
+{
+    OSKAR_B200_COORDS_F64 = 0,            /* oskar_grid_wproj.c:70-93, FP64 */
+    OSKAR_B200_COORDS_REFERENCE_F32 = 1   /* oskar_grid_wproj.c:168-204, float */
+};
+
+/* Storage type of the resident W-kernel cube. */
+enum
+{
+    OSKAR_B200_KERNEL_NATIVE = 0,  /* same as the data: FP32 or FP64 */
+    OSKAR_B200_KERNEL_F16 = 1,     /* FP16 with a per-plane scale */
+    OSKAR_B200_KERNEL_BF16 = 2     /* BF16 with a per-plane scale */
+};
+
+/* Grid accumulation for FP32 data. */
+enum
+{
+    OSKAR_B200_ACCUM_PLAIN = 0,        /* FP32 register sums, FP32 atomics */
+    OSKAR_B200_ACCUM_COMPENSATED = 1   /* FP32 grid plus an FP32 error grid */
+};
+
+typedef struct oskar_B200Options
+{
+    int coord_mode;      /* OSKAR_B200_COORDS_* */
+    int kernel_type;     /* OSKAR_B200_KERNEL_* */
+    int accum_mode;      /* OSKAR_B200_ACCUM_* */
+    int apply_weight;    /* 0: ignore weight (reference); 1: vis and norm x weight */
+    int classes_per_thread; /* 0: autotuned table; 1, 2 or 4 forces it */
+    int staging;         /* 0: auto; 1: TMA bulk copy to shared; 2: L1 reads */
+    int reserved[10];
+} oskar_B200Options;
+
+/* Fills the defaults (FP64 coordinates, native kernels, plain accumulation,
+ * weight ignored, autotuned launch shape). */
+OSKAR_B200_EXPORT void oskar_b200_options_init(oskar_B200Options* opt);
+
+/* Opaque workspace: a device, a set of grow-only device buffers and a
+ * default stream.  One workspace must not be used by two calls that can
+ * overlap in time; give each concurrent stream its own. */
+typedef struct oskar_B200Workspace oskar_B200Workspace;
+
+OSKAR_B200_EXPORT int oskar_b200_workspace_create(int device,
+        oskar_B200Workspace** ws);
+OSKAR_B200_EXPORT int oskar_b200_workspace_free(oskar_B200Workspace* ws);
+/* Bytes of device memory currently held by the workspace. */
+OSKAR_B200_EXPORT size_t oskar_b200_workspace_bytes(
+        const oskar_B200Workspace* ws);
+
+/* Opaque resident kernel cube: the W-kernels re-laid for the gridding
+ * kernel (per-plane, phase-major quadrant slabs in the chosen storage
+ * type) and the per-(plane, offset) norm table.  Build once, grid many. */
+typedef struct oskar_B200Cube oskar_B200Cube;
+
+/* conv_func: [num_w_planes][conv_size_half][conv_size_half][2] in the
+ * reference layout, FP32 (is_double = 0) or FP64 (is_double = 1), on the
+ * host (conv_func_on_device = 0) or device.  support[] is host memory.
+ * data_is_double selects the gridding precision the cube serves. */
+OSKAR_B200_EXPORT int oskar_b200_cube_create(oskar_B200Workspace* ws,
+        size_t num_w_planes, const int* support, int oversample,
+        int conv_size_half, const void* conv_func, int conv_func_is_double,
+        int conv_func_on_device, int data_is_double, int kernel_type,
+        void* stream, oskar_B200Cube** cube);
+OSKAR_B200_EXPORT int oskar_b200_cube_free(oskar_B200Cube* cube);
+OSKAR_B200_EXPORT size_t oskar_b200_cube_bytes(const oskar_B200Cube* cube);
+
+/* Grid num_points visibilities with a resident cube, asynchronously on
+ * `stream` (NULL: the workspace's stream).  uu, vv, ww, vis (interleaved),
+ * weight and grid are DEVICE pointers of the cube's data precision (float
+ * or double).  d_num_skipped (device, uint64) is overwritten with this
+ * call's skip count; d_norm (device, double) is incremented.  Either may be
+ * NULL.  The grid accumulates. */
+OSKAR_B200_EXPORT int oskar_b200_grid(oskar_B200Workspace* ws,
+        const oskar_B200Cube* cube, const oskar_B200Options* opt,
+        size_t num_points, const void* uu, const void* vv, const void* ww,
+        const void* vis, const void* weight, double cell_size_rad,
+        double w_scale, int grid_size, void* grid,
+        unsigned long long* d_num_skipped, double* d_norm, void* stream);
+
+/* The compensation (error) grid used by OSKAR_B200_ACCUM_COMPENSATED lives
+ * in the workspace; this adds it into `grid` (FP32, device) and clears it. */
+OSKAR_B200_EXPORT int oskar_b200_fold_compensation(oskar_B200Workspace* ws,
+        void* grid, int grid_size, void* stream);
+
+/* Per-visibility placement exactly as the gridder computes it (device
+ * pointers, int32 outputs, any may be NULL): grid cell, clamped w-plane,
+ * oversample offsets, conjugation sign (+1/-1) and skip flag (0/1). */
+OSKAR_B200_EXPORT int oskar_b200_place(oskar_B200Workspace* ws,
+        int data_is_double, int coord_mode, size_t num_w_planes,
+        const int* support, int oversample, size_t num_points,
+        const void* uu, const void* vv, const void* ww,
+        double cell_size_rad, double w_scale, int grid_size,
+        int32_t* gu, int32_t* gv, int32_t* plane, int32_t* off_u,
+        int32_t* off_v, int32_t* conj, int32_t* skipped, void* stream);
+
+/* Statistics of the most recent oskar_b200_grid call on this workspace
+ * (valid once its stream has been synchronised). */
+typedef struct oskar_B200Stats
+{
+    unsigned long long num_points;     /* visibilities given */
+    unsigned long long num_gridded;    /* not skipped */
+    unsigned long long grid_updates;   /* sum of (2S+1)^2 over gridded */
+    unsigned long long num_tasks;      /* gridding work items */
+    unsigned long long atomic_flushes; /* grid atomics issued */
+    int status;                        /* device-side check status */
+    int kernel_launches;               /* kernels the call launched */
+    /* Stage durations in ms (CUDA events on the call's stream), filled
+     * when stage timing is enabled on the workspace, else 0: placement and
+     * keys, radix sort, permutation and task list, gridding kernel. */
+    float prep_ms, sort_ms, tasks_ms, grid_ms;
+} oskar_B200Stats;
+
+OSKAR_B200_EXPORT int oskar_b200_last_stats(oskar_B200Workspace* ws,
+        oskar_B200Stats* stats);
+
+/* Records CUDA events between the stages of every later oskar_b200_grid
+ * call on this workspace (enable = 1) or stops doing so (0). */
+OSKAR_B200_EXPORT int oskar_b200_set_stage_timing(oskar_B200Workspace* ws,
+        int enable);
+
+/* Measures the device's complex-FP32 grid-atomic rate: `iters` rounds in
+ * which every warp of a persistent grid issues red.global.add.v2.f32 to 32
+ * consecutive cells at a pseudo-random row of `grid` (grid_size^2 complex
+ * FP32 cells, device memory, contents destroyed).  Synchronous; returns
+ * complex updates per second in *updates_per_s. */
+OSKAR_B200_EXPORT int oskar_b200_measure_atomic_rate(oskar_B200Workspace* ws,
+        void* grid, int grid_size, int iters, double* updates_per_s);
+
+/* Library build description (arch, version). */
+OSKAR_B200_EXPORT const char* oskar_b200_build_info(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OSKAR_GRID_WPROJ_B200_H_ */

@@ -1,0 +1,224 @@
+"""ctypes front end for the CPU checker libraries.
+
+TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline leg import this module.  It wraps:
+
+  liboracle.so             the C restatement in oracle.c (always built), and
+  _ref/libref_gridder.so   the reference's oskar_grid_wproj.c and
+                           oskar_grid_weights.c compiled unmodified
+                           (present where the reference sources were
+                           available at build time).
+
+Build both with `make -C oracle`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libref_gridder.so")
+
+_P = C.c_void_p
+_SZ = C.c_size_t
+
+_GRID_ARGS_D = [_SZ, _P, C.c_int, C.c_int, _P, _SZ, _P, _P, _P, _P, _P,
+                C.c_double, C.c_double, C.c_int, _P, _P, _P]
+_GRID_ARGS_F = [_SZ, _P, C.c_int, C.c_int, _P, _SZ, _P, _P, _P, _P, _P,
+                C.c_float, C.c_float, C.c_int, _P, _P, _P]
+GRID_FN_D = C.CFUNCTYPE(None, *_GRID_ARGS_D)
+GRID_FN_F = C.CFUNCTYPE(None, *_GRID_ARGS_F)
+
+_oracle = None
+_ref = None
+
+
+def build(quiet: bool = True) -> None:
+    """Compile liboracle.so (and _ref/ where the reference sources exist)."""
+    out = subprocess.run(["make", "-C", HERE, "all"], capture_output=True,
+                         text=True)
+    if out.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
+    if not quiet:
+        print(out.stdout)
+
+
+def _declare(lib, prefix):
+    for suffix, args in (("grid_wproj_d", _GRID_ARGS_D),
+                         ("grid_wproj_f", _GRID_ARGS_F)):
+        fn = getattr(lib, prefix + suffix)
+        fn.argtypes = args
+        fn.restype = None
+    return lib
+
+
+def oracle_lib():
+    """The C restatement (builds it on first use if missing)."""
+    global _oracle
+    if _oracle is None:
+        if not os.path.exists(ORACLE_SO):
+            build()
+        lib = _declare(C.CDLL(ORACLE_SO), "orc_")
+        pl = [_SZ, _P, C.c_int, _SZ, _P, _P, _P]
+        lib.orc_vis_place_d.argtypes = pl + [C.c_double, C.c_double, C.c_int] + [_P] * 8
+        lib.orc_vis_place_f.argtypes = pl + [C.c_float, C.c_float, C.c_int] + [_P] * 8
+        lib.orc_vis_place_d.restype = lib.orc_vis_place_f.restype = None
+        lib.orc_grid_wproj_d_banded.argtypes = _GRID_ARGS_D + [C.c_int]
+        lib.orc_grid_wproj_f_banded.argtypes = _GRID_ARGS_F + [C.c_int]
+        lib.orc_count_taps_d.argtypes = [_SZ, _P, C.c_int, _SZ, _P, _P, _P,
+                                         C.c_double, C.c_double, C.c_int]
+        lib.orc_count_taps_d.restype = C.c_uint64
+        for t, fa in (("d", (C.c_double, _GRID_ARGS_D)),
+                      ("f", (C.c_float, _GRID_ARGS_F))):
+            fn = getattr(lib, "orc_time_parallel_" + t)
+            fn.argtypes = [_P, C.c_int, _SZ] + fa[1][:13] + [_P, _P, _P]
+            fn.restype = C.c_double
+            w = getattr(lib, "orc_grid_weights_write_" + t)
+            w.argtypes = [_SZ, _P, _P, _P, fa[0], C.c_int, _P, _P]
+            r = getattr(lib, "orc_grid_weights_read_" + t)
+            r.argtypes = [_SZ, _P, _P, _P, _P, fa[0], C.c_int, _P, _P]
+            w.restype = r.restype = None
+        _oracle = lib
+    return _oracle
+
+
+def reference_lib():
+    """The reference compiled from its own sources, or None if not built."""
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF_SO):
+            return None
+        lib = _declare(C.CDLL(REF_SO), "ref_oskar_")
+        for t, real in (("d", C.c_double), ("f", C.c_float)):
+            w = getattr(lib, "ref_oskar_grid_weights_write_" + t)
+            w.argtypes = [_SZ, _P, _P, _P, real, C.c_int, _P, _P]
+            r = getattr(lib, "ref_oskar_grid_weights_read_" + t)
+            r.argtypes = [_SZ, _P, _P, _P, _P, real, C.c_int, _P, _P]
+            w.restype = r.restype = None
+        _ref = lib
+    return _ref
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_P) if a is not None else None
+
+
+def _arrays(w: dict, dtype):
+    """Contiguous arrays of one dtype from a Workload.numpy() dict."""
+    conv = lambda k: np.ascontiguousarray(w[k], dtype=dtype)
+    return dict(support=np.ascontiguousarray(w["support"], dtype=np.int32),
+                conv_func=conv("conv_func"), uu=conv("uu"), vv=conv("vv"),
+                ww=conv("ww"), vis=conv("vis"), weight=conv("weight"))
+
+
+def grid(fn, w: dict, dtype, grid_arr=None, norm: float = 0.0,
+         threads: int | None = None):
+    """Call a gridding function with the reference's signature on the arrays
+    of `w`.  Returns (num_skipped, norm, grid)."""
+    a = _arrays(w, dtype)
+    g = w["grid_size"]
+    if grid_arr is None:
+        grid_arr = np.zeros(2 * g * g, dtype=dtype)
+    skipped = C.c_size_t(0)
+    nrm = C.c_double(norm)
+    args = [w["num_w_planes"], _ptr(a["support"]), w["oversample"],
+            w["conv_size_half"], _ptr(a["conv_func"]), a["uu"].shape[0],
+            _ptr(a["uu"]), _ptr(a["vv"]), _ptr(a["ww"]), _ptr(a["vis"]),
+            _ptr(a["weight"]), w["cell_size_rad"], w["w_scale"], g,
+            C.byref(skipped), C.byref(nrm), _ptr(grid_arr)]
+    if threads is not None:
+        args.append(threads)
+    fn(*args)
+    return skipped.value, nrm.value, grid_arr
+
+
+def grid_d(w, grid_arr=None, norm=0.0, threads=None):
+    """Oracle FP64 gridding (banded threads when `threads` is given)."""
+    lib = oracle_lib()
+    fn = lib.orc_grid_wproj_d if threads is None else lib.orc_grid_wproj_d_banded
+    return grid(fn, w, np.float64, grid_arr, norm, threads)
+
+
+def grid_f(w, grid_arr=None, norm=0.0, threads=None):
+    """Oracle FP32 gridding with the reference's float coordinates."""
+    lib = oracle_lib()
+    fn = lib.orc_grid_wproj_f if threads is None else lib.orc_grid_wproj_f_banded
+    return grid(fn, w, np.float32, grid_arr, norm, threads)
+
+
+def place(w: dict, single: bool = False):
+    """Per-visibility (gu, gv, plane, raw_plane, off_u, off_v, conj, skipped)
+    with FP64 coordinates, or the reference _f's float ones if single."""
+    lib = oracle_lib()
+    dt = np.float32 if single else np.float64
+    a = _arrays(w, dt)
+    n = a["uu"].shape[0]
+    outs = [np.zeros(n, np.int32) for _ in range(6)] + \
+        [np.zeros(n, np.int8), np.zeros(n, np.uint8)]
+    fn = lib.orc_vis_place_f if single else lib.orc_vis_place_d
+    fn(w["num_w_planes"], _ptr(a["support"]), w["oversample"], n,
+       _ptr(a["uu"]), _ptr(a["vv"]), _ptr(a["ww"]), w["cell_size_rad"],
+       w["w_scale"], w["grid_size"], *[_ptr(o) for o in outs])
+    keys = ("gu", "gv", "plane", "raw_plane", "off_u", "off_v", "conj",
+            "skipped")
+    return dict(zip(keys, outs))
+
+
+def count_taps(w: dict) -> int:
+    lib = oracle_lib()
+    a = _arrays(w, np.float64)
+    return int(lib.orc_count_taps_d(
+        w["num_w_planes"], _ptr(a["support"]), w["oversample"],
+        a["uu"].shape[0], _ptr(a["uu"]), _ptr(a["vv"]), _ptr(a["ww"]),
+        w["cell_size_rad"], w["w_scale"], w["grid_size"]))
+
+
+def time_parallel(w: dict, single: bool, threads: int, use_reference: bool,
+                  want_grid: bool = False):
+    """Time the reference's gridder (use_reference) or the restatement on
+    `threads` threads with private grids.  The reference's FP32 function
+    always processes exactly 10000 points (oskar_grid_wproj.c:155), so it is
+    driven in consecutive 10000-point calls.  Returns
+    (seconds, num_skipped, norm, grid or None)."""
+    dt = np.float32 if single else np.float64
+    a = _arrays(w, dt)
+    g = w["grid_size"]
+    out = np.zeros(2 * g * g, dtype=dt) if want_grid else None
+    if use_reference:
+        ref = reference_lib()
+        if ref is None:
+            raise RuntimeError("reference library not built (oracle/_ref)")
+        fn = ref.ref_oskar_grid_wproj_f if single else ref.ref_oskar_grid_wproj_d
+        chunk = 10000 if single else 0
+    else:
+        lib = oracle_lib()
+        fn = lib.orc_grid_wproj_f if single else lib.orc_grid_wproj_d
+        chunk = 0
+    fnp = C.cast(fn, _P)
+    skipped = C.c_size_t(0)
+    nrm = C.c_double(0.0)
+    timer = oracle_lib().orc_time_parallel_f if single else \
+        oracle_lib().orc_time_parallel_d
+    secs = timer(fnp, threads, chunk, w["num_w_planes"], _ptr(a["support"]),
+                 w["oversample"], w["conv_size_half"], _ptr(a["conv_func"]),
+                 a["uu"].shape[0], _ptr(a["uu"]), _ptr(a["vv"]),
+                 _ptr(a["ww"]), _ptr(a["vis"]), _ptr(a["weight"]),
+                 w["cell_size_rad"], w["w_scale"], g, C.byref(skipped),
+                 C.byref(nrm), _ptr(out))
+    if secs < 0:
+        raise MemoryError("CPU baseline could not allocate private grids")
+    return secs, skipped.value, nrm.value, out
+
+
+def rel_rms(test: np.ndarray, ref: np.ndarray) -> float:
+    """The reference harness's grid error metric (main.cpp:575-598):
+    sqrt(sum |test - ref|^2) / sqrt(sum |ref|^2), accumulated in FP64."""
+    t = np.asarray(test, dtype=np.float64)
+    r = np.asarray(ref, dtype=np.float64)
+    den = np.sqrt(np.sum(r * r))
+    num = np.sqrt(np.sum((t - r) ** 2))
+    return float(num / den) if den > 0 else float(num)

@@ -1,0 +1,45 @@
+import glob
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+GOLDEN_DIR = os.path.join(ROOT, "tests", "golden")
+
+
+def pytest_configure(config):
+    config.addinivalue_line(
+        "markers", "gpu: needs a B200 (runs the CUDA gridder)")
+
+
+def golden_names():
+    return sorted(os.path.splitext(os.path.basename(p))[0]
+                  for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz")))
+
+
+def load_golden(name):
+    """A fixture as (inputs dict in the reference convention, outputs)."""
+    z = np.load(os.path.join(GOLDEN_DIR, name + ".npz"))
+    single = bool(z["single"])
+    inputs = dict(num_w_planes=int(z["num_w_planes"]), support=z["support"],
+                  oversample=int(z["oversample"]),
+                  conv_size_half=int(z["conv_size_half"]),
+                  conv_func=z["conv_func"], uu=z["uu"], vv=z["vv"],
+                  ww=z["ww"], vis=z["vis"], weight=z["weight"],
+                  cell_size_rad=float(z["cell_size_rad"]),
+                  w_scale=float(z["w_scale"]), grid_size=int(z["grid_size"]))
+    out = dict(grid=z["out_grid"], norm=float(z["out_norm"]),
+               skipped=int(z["out_skipped"]), single=single)
+    return inputs, out
+
+
+@pytest.fixture(scope="session")
+def oracle():
+    from oracle import oracle as O
+    O.oracle_lib()
+    return O

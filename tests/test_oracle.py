@@ -1,0 +1,148 @@
+"""The CPU oracle is pinned to the reference: bit-exact against the
+reference's own gridder compiled from its sources (oracle/_ref) and against
+the golden fixtures generated from it."""
+import numpy as np
+import pytest
+
+from conftest import golden_names, load_golden
+from fpga_gridding_b200 import workloads as W
+
+
+@pytest.fixture(scope="module")
+def small():
+    return W.plain_small().numpy()
+
+
+@pytest.fixture(scope="module")
+def ref(oracle):
+    lib = oracle.reference_lib()
+    if lib is None:
+        pytest.skip("reference not compiled here (oracle/_ref missing)")
+    return lib
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_oracle_matches_golden_bit_exact(oracle, name):
+    inputs, out = load_golden(name)
+    fn = oracle.grid_f if out["single"] else oracle.grid_d
+    skipped, norm, grid = fn(inputs)
+    assert skipped == out["skipped"]
+    assert norm == out["norm"]
+    assert np.array_equal(grid, out["grid"])
+
+
+def test_oracle_d_matches_reference_full_small_config(oracle, ref, small):
+    s1, n1, g1 = oracle.grid(ref.ref_oskar_grid_wproj_d, small, np.float64)
+    s2, n2, g2 = oracle.grid_d(small)
+    assert (s1, n1) == (s2, n2)
+    assert np.array_equal(g1, g2)
+
+
+def test_oracle_f_matches_reference_on_10000_point_slices(oracle, ref, small):
+    # The shipped FP32 reference grids exactly 10000 points per call
+    # (oskar_grid_wproj.c:155); compare slice by slice, accumulating.
+    g = small["grid_size"]
+    g1 = np.zeros(2 * g * g, np.float32)
+    g2 = np.zeros(2 * g * g, np.float32)
+    n1 = n2 = 0.0
+    for start in (0, 10000, 120000, 230000):
+        part = dict(small)
+        for k in ("uu", "vv", "ww", "weight"):
+            part[k] = small[k][start:start + 10000]
+        part["vis"] = small["vis"][2 * start:2 * (start + 10000)]
+        s1, n1, g1 = oracle.grid(ref.ref_oskar_grid_wproj_f, part, np.float32,
+                                 g1, n1)
+        s2, n2, g2 = oracle.grid_f(part, g2, n2)
+        assert s1 == s2
+    assert n1 == n2
+    assert np.array_equal(g1, g2)
+
+
+def test_banded_threads_bit_identical_to_serial(oracle, small):
+    s1, n1, g1 = oracle.grid_d(small)
+    for t in (1, 3, 8):
+        s2, n2, g2 = oracle.grid_d(small, threads=t)
+        assert (s1, n1) == (s2, n2)
+        assert np.array_equal(g1, g2)
+    inputs, _ = load_golden("edges_d")
+    s1, n1, g1 = oracle.grid_d(inputs)
+    s2, n2, g2 = oracle.grid_d(inputs, threads=5)
+    assert (s1, n1) == (s2, n2) and np.array_equal(g1, g2)
+    fs1, fn1, fg1 = oracle.grid_f(small)
+    fs2, fn2, fg2 = oracle.grid_f(small, threads=4)
+    assert (fs1, fn1) == (fs2, fn2) and np.array_equal(fg1, fg2)
+
+
+def test_known_answer_all_ones(oracle):
+    """FAKE_VIS_VALUES / FAKE_KERNEL_VALUES mode (Defines.h:37-38): every
+    kept point adds 1 to each footprint cell and (2S+1)^2 to norm."""
+    inputs, out = load_golden("ones_d")
+    p = oracle.place(inputs)
+    keep = p["skipped"] == 0
+    s = inputs["support"][p["plane"][keep]]
+    assert out["norm"] == float(np.sum((2 * s + 1) ** 2))
+    g = inputs["grid_size"]
+    expect = np.zeros((g, g))
+    for gu, gv, sp in zip(p["gu"][keep], p["gv"][keep], s):
+        expect[gv - sp:gv + sp + 1, gu - sp:gu + sp + 1] += 1.0
+    grid = out["grid"].reshape(g, g, 2)
+    assert np.array_equal(grid[..., 0], expect)
+    assert not grid[..., 1].any()
+
+
+def test_placement_edge_cases(oracle):
+    inputs, out = load_golden("edges_d")
+    p = oracle.place(inputs)
+    assert int(p["skipped"].sum()) == out["skipped"]
+    # half-way cell rounding is away from zero: u = 0.5 -> pos_u = -0.5
+    # -> round -> -1 -> grid_u = 31
+    assert p["gu"][0] == 31
+    # plane clamp: w = -100 -> round(10) clamps to the last plane (3)
+    assert p["raw_plane"][4] == 10 and p["plane"][4] == 3
+    # conjugation only for w > 0
+    assert p["conj"][1] == -1 and p["conj"][0] == 1 and p["conj"][2] == 1
+    # offsets stay within [-os/2, os/2]
+    assert np.abs(p["off_u"][p["skipped"] == 0]).max() <= 2
+
+
+def test_float_coordinates_differ_from_double_only_rarely(oracle, small):
+    pd = oracle.place(small)
+    pf = oracle.place(small, single=True)
+    diff = sum(int((pd[k] != pf[k]).sum()) for k in ("gu", "gv", "plane"))
+    assert diff < small["uu"].size * 1e-3
+
+
+def test_weights_restatement_matches_reference(oracle, ref, small):
+    import ctypes as C
+    n = small["uu"].size
+    g = small["grid_size"]
+    for real, t in ((np.float64, "d"), (np.float32, "f")):
+        uu = small["uu"].astype(real)
+        vv = small["vv"].astype(real)
+        w1 = np.ones(n, real)
+        outs = []
+        for lib, prefix in ((ref, "ref_oskar_"), (oracle.oracle_lib(), "orc_")):
+            grid = np.zeros(g * g, real)
+            sk = C.c_size_t(0)
+            getattr(lib, prefix + "grid_weights_write_" + t)(
+                n, uu.ctypes.data, vv.ctypes.data, w1.ctypes.data,
+                small["cell_size_rad"], g, C.byref(sk), grid.ctypes.data)
+            wout = np.zeros(n, real)
+            sk2 = C.c_size_t(0)
+            getattr(lib, prefix + "grid_weights_read_" + t)(
+                n, uu.ctypes.data, vv.ctypes.data, w1.ctypes.data,
+                wout.ctypes.data, small["cell_size_rad"], g, C.byref(sk2),
+                grid.ctypes.data)
+            outs.append((sk.value, sk2.value, grid, wout))
+        assert outs[0][:2] == outs[1][:2]
+        assert np.array_equal(outs[0][2], outs[1][2])
+        assert np.array_equal(outs[0][3], outs[1][3])
+
+
+def test_parallel_timing_harness_sums_to_serial(oracle, small):
+    secs, sk, nrm, grid = oracle.time_parallel(small, False, 3, False,
+                                               want_grid=True)
+    s1, n1, g1 = oracle.grid_d(small)
+    assert secs > 0 and sk == s1
+    assert abs(nrm - n1) <= 1e-12 * abs(n1)
+    assert oracle.rel_rms(grid, g1) < 1e-13
