@@ -132,7 +132,7 @@ int validate_cube_args(size_t num_w_planes, const int* support,
                        const void* conv_func)
 {
     if (num_w_planes == 0 || num_w_planes > (1u << 15) || !support ||
-        !conv_func || oversample < 1 || oversample > 64 ||
+        !conv_func || oversample < 1 || oversample > 32 ||
         conv_size_half < 1)
         return OSKAR_B200_ERR_INVALID_ARGUMENT;
     const long long csh = conv_size_half;
@@ -141,7 +141,10 @@ int validate_cube_args(size_t num_w_planes, const int* support,
     for (size_t p = 0; p < num_w_planes; ++p)
     {
         const long long s = support[p];
-        if (s < 0 || s > 4096) return OSKAR_B200_ERR_INVALID_ARGUMENT;
+        if (s < 0) return OSKAR_B200_ERR_INVALID_ARGUMENT;
+        // The gridding kernel lays a footprint's 2S+1 columns across one
+        // 256-thread CTA.
+        if (s > 127) return OSKAR_B200_ERR_UNSUPPORTED;
         // Largest flat index the reference reads on this plane
         // (oskar_grid_wproj.c:110-116) must lie inside the cube.
         const long long e = oversample * s + half;

@@ -77,24 +77,27 @@ __global__ void plane_maxabs_kernel(const IN* __restrict__ cube,
 template <typename IN, typename KT>
 __global__ void relayout_kernel(const IN* __restrict__ cube,
                                 const PlaneDesc* __restrict__ planes,
-                                int oversample, int conv_size_half,
+                                int oversample, int half, int conv_size_half,
                                 KT* __restrict__ slabs)
 {
     const int p = blockIdx.y;
     const PlaneDesc d = planes[p];
     const long long base = (long long)p * conv_size_half * conv_size_half;
-    const int total = d.pitch * d.pitch;
+    const int w = 2 * d.support + 1;
+    const int total = d.rows * d.pitch;
     const float inv = 1.0f / d.scale;
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total;
          e += gridDim.x * blockDim.x)
     {
         const int row = e / d.pitch, col = e % d.pitch;
-        // position = (x % os) * L + x / os  <=>  x = (pos % L) * os + pos / L
-        const int xv = (row % d.L) * oversample + row / d.L;
+        // row = (off_v + H) * W + (j + S)  ->  quadrant row |off_v + j * os|
+        const int off_v = row / w - half, j = row % w - d.support;
+        const int xv = abs(off_v + j * oversample);
+        // column position = (x % os) * L + x / os  <=>
+        // x = (pos % L) * os + pos / L
         const int xu = (col % d.L) * oversample + col / d.L;
         double re = 0.0, im = 0.0;
-        if (xv < d.extent && xu < d.extent && row / d.L < oversample &&
-            col / d.L < oversample)
+        if (xu < d.extent)
         {
             const long long f = base + (long long)xv * conv_size_half + xu;
             re = (double)cube[2 * f];
@@ -141,7 +144,7 @@ void launch_relayout(const oskar_B200Cube* c, const void* conv,
     relayout_kernel<IN, KT><<<grid, 256, 0, st>>>(
         static_cast<const IN*>(conv),
         static_cast<const PlaneDesc*>(c->d_planes.ptr), c->oversample,
-        c->conv_size_half, static_cast<KT*>(c->d_slabs.ptr));
+        c->half, c->conv_size_half, static_cast<KT*>(c->d_slabs.ptr));
 }
 
 }  // namespace
@@ -160,8 +163,9 @@ int cube_build(oskar_B200Cube* c, const void* d_conv, int conv_is_double,
         d.extent = os * d.support + c->half + 1;
         d.L = (d.extent + os - 1) / os;
         d.pitch = os * d.L;
+        d.rows = (2 * c->half + 1) * (2 * d.support + 1);
         d.offset = off;
-        const size_t elems = (size_t)d.pitch * d.pitch;
+        const size_t elems = (size_t)d.rows * d.pitch;
         const size_t padded = (elems + align_elems - 1) / align_elems *
                               align_elems;
         d.bytes = (unsigned)(padded * c->elem_bytes);

@@ -18,6 +18,7 @@
 //   grid[v][u] += vis * (conj ? conj(K) : K)(|off_v + j*os|, |off_u + k*os|)
 // (oskar_grid_wproj.c:104-123), summed in a different order.
 #include <algorithm>
+#include <mutex>
 
 #include "common.cuh"
 #include "grid_romein.cuh"
@@ -32,15 +33,15 @@ template <> struct Vec2<double> { using type = double2; };
 
 // Per-visibility tap record.  For a class (a, b) of a task with footprint W:
 //   ru = (a + mu) mod W, rv = (b + mv) mod W   (offsets inside the footprint)
-//   column = ru >= tu ? cp + ru : cn - ru      (slab position, see PlaneDesc)
-//   rowoff = rv >= tv ? rp + rv * pitch : rn - rv * pitch
-//   cell   = origin + ru + rv * grid_size
+//   column = ru >= tu ? cp + ru : cn - ru      (slab column, see PlaneDesc)
+//   kernel index = rowbase + column + rv * pitch
+//   cell         = origin + ru + rv * grid_size
 template <typename GT>
 struct __align__(16) TapVis
 {
     unsigned origin;
-    int mu, mv, tuv;   // tuv = tu | tv << 16
-    int cp, cn, rp, rn;
+    int mu, mv, tu;
+    int cp, cn, rowbase, unused;
     GT ar, ai, bi, br; // re += ar*Kre - ai*Kim; im += bi*Kre + br*Kim
 };
 
@@ -48,7 +49,8 @@ template <typename GT>
 __device__ __forceinline__ TapVis<GT> derive(const int4 rec,
                                              const typename Vec2<GT>::type vis,
                                              const PlaneDesc& d, int grid_size,
-                                             int oversample, int half)
+                                             int oversample, int half,
+                                             unsigned long long* status)
 {
     TapVis<GT> t;
     const int s = d.support, w = 2 * s + 1, os = oversample;
@@ -61,17 +63,26 @@ __device__ __forceinline__ TapVis<GT> derive(const int4 rec,
     t.origin = (unsigned)u0 + (unsigned)v0 * (unsigned)grid_size;
     t.mu = (w - u0 % w) % w;
     t.mv = (w - v0 % w) % w;
-    // Taps k >= k0 have off + k*os >= 0 (the ascending run of positions).
-    const int tu = s + (off_u < 0 ? 1 : 0);
-    const int tv = s + (off_v < 0 ? 1 : 0);
-    t.tuv = tu | (tv << 16);
+    // Column taps k >= 0 (k >= 1 when off_u < 0) have off_u + k*os >= 0:
+    // the ascending run of slab columns.
+    t.tu = s + (off_u < 0 ? 1 : 0);
     const int rpu = ((off_u % os) + os) % os, rnu = ((-off_u % os) + os) % os;
-    const int rpv = ((off_v % os) + os) % os, rnv = ((-off_v % os) + os) % os;
     t.cp = rpu * d.L + (off_u - rpu) / os - s;
     t.cn = rnu * d.L + (-off_u - rnu) / os + s;
-    t.rp = (rpv * d.L + (off_v - rpv) / os - s) * d.pitch;
-    t.rn = (rnv * d.L + (-off_v - rnv) / os + s) * d.pitch;
-    const GT sc = (GT)d.scale;
+    // First of the W slab rows holding this row offset's taps.
+    t.rowbase = (off_v + half) * w * d.pitch;
+    t.unused = 0;
+    GT sc = (GT)d.scale;
+    // The prep kernel only keeps points whose footprint lies inside the
+    // grid; a record that breaks this is reported and neutralised (zero
+    // weight at cell 0) so no flush can leave the grid.
+    if (u0 < 0 || v0 < 0 || u0 + w > grid_size || v0 + w > grid_size)
+    {
+        atomicOr(status, (unsigned long long)DEV_ERR_GRID_INDEX);
+        t.origin = 0;
+        t.mu = t.mv = 0;
+        sc = GT(0);
+    }
     const GT vr = vis.x * sc, vi = vis.y * sc;
     t.ar = vr;
     t.ai = conj * vi;
@@ -80,14 +91,113 @@ __device__ __forceinline__ TapVis<GT> derive(const int4 rec,
     return t;
 }
 
-template <typename GT>
-__device__ __forceinline__ void flush(GT* grid, unsigned cell, unsigned cells,
-                                      GT re, GT im, unsigned long long* status)
+// Spreads the low 9 bits of x to the even bit positions.
+__device__ __forceinline__ uint32_t spread9(uint32_t x)
 {
-    if (cell < cells)
-        red_add_c(grid + 2 * (size_t)cell, re, im);
+    x &= 0x1ffu;
+    x = (x | (x << 8)) & 0x00ff00ffu;
+    x = (x | (x << 4)) & 0x0f0f0f0fu;
+    x = (x | (x << 2)) & 0x33333333u;
+    x = (x | (x << 1)) & 0x55555555u;
+    return x;
+}
+
+// Returns, for thread t < m, the task-relative index of the t-th
+// visibility in (row offset, Morton cell) order.  Bitonic sort of one key
+// per thread: key = (off_v + half) << 26 | Morton(gu, gv low 9 bits) << 8 |
+// index (m <= 256, half <= 16); strides below 32 use warp shuffles, larger
+// ones go through shared memory.  All threads of the CTA must call it.
+__device__ __forceinline__ int task_order(const int4* __restrict__ srec,
+                                          uint32_t begin, int m,
+                                          uint32_t* s_order)
+{
+    static_assert(kTaskMax == kGridThreads, "one key per thread");
+    const unsigned t = threadIdx.x;
+    uint32_t key = 0xffffffffu;
+    if ((int)t < m)
+    {
+        const int4 r = srec[begin + t];
+        key = ((uint32_t)(r.w >> 16) << 26) |
+              ((spread9((uint32_t)r.x) | (spread9((uint32_t)r.y) << 1)) << 8) |
+              t;
+    }
+#pragma unroll
+    for (unsigned k = 2; k <= (unsigned)kGridThreads; k <<= 1)
+    {
+#pragma unroll
+        for (unsigned j = k >> 1; j > 0; j >>= 1)
+        {
+            uint32_t other;
+            if (j >= 32)
+            {
+                s_order[t] = key;
+                __syncthreads();
+                other = s_order[t ^ j];
+                __syncthreads();
+            }
+            else
+            {
+                other = __shfl_xor_sync(0xffffffffu, key, j);
+            }
+            const bool ascending = (t & k) == 0;
+            const bool take_min = ((t & j) == 0) == ascending;
+            key = take_min ? min(key, other) : max(key, other);
+        }
+    }
+    return (int)(key & 0xffu);
+}
+
+// Predicated complex flush: one vector reduction when `pred` holds, no
+// branch (the flush decision differs from lane to lane on most taps).
+__device__ __forceinline__ void red_add_c_if(bool pred, float* addr, float re,
+                                             float im)
+{
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %3, 0;\n\t"
+                 "@p red.relaxed.gpu.global.add.v2.f32 [%0], {%1, %2};\n\t}"
+                 :: "l"(addr), "f"(re), "f"(im), "r"((int)pred) : "memory");
+}
+
+__device__ __forceinline__ void red_add_c_if(bool pred, double* addr,
+                                             double re, double im)
+{
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %3, 0;\n\t"
+                 "@p red.relaxed.gpu.global.add.f64 [%0], %1;\n\t"
+                 "@p red.relaxed.gpu.global.add.f64 [%4], %2;\n\t}"
+                 :: "l"(addr), "d"(re), "d"(im), "r"((int)pred), "l"(addr + 1)
+                 : "memory");
+}
+
+// Thread layout of one task.  The W x W classes are split into W columns
+// (a) and W rows (b).  A thread owns one column and CPT rows, so the column
+// arithmetic of a tap is done once per visibility and shared by its CPT
+// classes, and the 32 lanes of a warp hold consecutive columns (contiguous
+// kernel reads, coalesced flushes).  `groups` threads share a column per
+// slice; thread g of a column takes rows g, g + groups, ... (CPT of them per
+// pass).  When the footprint is small, `slices` independent copies of the
+// layout split the task's visibilities between them.
+struct TaskLayout
+{
+    int groups, passes, slices;
+};
+
+template <int CPT>
+__device__ __forceinline__ TaskLayout task_layout(int w)
+{
+    TaskLayout t;
+    const int need = (w + CPT - 1) / CPT;
+    if (w * need <= kGridThreads)
+    {
+        t.groups = need;
+        t.passes = 1;
+        t.slices = kGridThreads / (w * need);
+    }
     else
-        atomicOr(status, (unsigned long long)DEV_ERR_GRID_INDEX);
+    {
+        t.groups = kGridThreads / w;
+        t.passes = (w + t.groups * CPT - 1) / (t.groups * CPT);
+        t.slices = 1;
+    }
+    return t;
 }
 
 // One task: every class of the W x W footprint over the task's visibilities.
@@ -97,61 +207,57 @@ __device__ __forceinline__ void process_task(const TapVis<GT>* __restrict__ s_vi
                                              const KT* __restrict__ slab,
                                              GT* __restrict__ grid,
                                              int grid_size, unsigned cells,
-                                             unsigned long long* status,
                                              unsigned& flushes)
 {
-    const int classes = w * w;
-    const int tps = min(kGridThreads, (classes + CPT - 1) / CPT);
-    int slices = kGridThreads / tps;
-    if (slices > m) slices = m;
-    const int r = threadIdx.x / tps, l = threadIdx.x - r * tps;
+    const TaskLayout lay = task_layout<CPT>(w);
+    const int per_slice = w * lay.groups;
+    int slices = lay.slices < m ? lay.slices : m;
+    const int r = threadIdx.x / per_slice;
     if (r >= slices) return;
+    const int l = threadIdx.x - r * per_slice;
+    const int a = l % w, g = l / w;
     const int i0 = (r * m) / slices, i1 = ((r + 1) * m) / slices;
-    const int per_pass = tps * CPT;
-    for (int base = 0; base < classes; base += per_pass)
+    for (int pass = 0; pass < lay.passes; ++pass)
     {
-        int ca[CPT], cb[CPT];
-        bool act[CPT];
+        const int b0 = pass * lay.groups * CPT + g;
         GT are[CPT], aim[CPT];
         unsigned cur[CPT];
 #pragma unroll
         for (int q = 0; q < CPT; ++q)
         {
-            const int c = base + q * tps + l;
-            act[q] = c < classes;
-            const int cc = act[q] ? c : 0;
-            cb[q] = cc / w;
-            ca[q] = cc - cb[q] * w;
             are[q] = aim[q] = GT(0);
             cur[q] = 0xffffffffu;
         }
+        // Rows of this thread in this pass: b0 + q * groups, q < rows_here.
+        int rows_here = (w - b0 + lay.groups - 1) / lay.groups;
+        rows_here = rows_here < 0 ? 0 : (rows_here > CPT ? CPT : rows_here);
         for (int i = i0; i < i1; ++i)
         {
             const TapVis<GT> v = s_vis[i];
-            const int tu = v.tuv & 0xffff, tv = v.tuv >> 16;
+            // (a + mu) mod W for a + mu in [0, 2W): min over unsigned wraps
+            const unsigned ru = min((unsigned)(a + v.mu),
+                                    (unsigned)(a + v.mu - w));
+            const int col = (int)ru >= v.tu ? v.cp + (int)ru : v.cn - (int)ru;
+            const int kbase = v.rowbase + col;
+            const unsigned cell0 = v.origin + ru;
 #pragma unroll
             for (int q = 0; q < CPT; ++q)
             {
-                if (!act[q]) continue;
-                int ru = ca[q] + v.mu;
-                ru = ru >= w ? ru - w : ru;
-                int rv = cb[q] + v.mv;
-                rv = rv >= w ? rv - w : rv;
-                const int col = ru >= tu ? v.cp + ru : v.cn - ru;
-                const int roff = rv >= tv ? v.rp + rv * pitch : v.rn - rv * pitch;
-                const auto k = KernelLoad<KT>::get(slab[roff + col]);
-                const unsigned cell = v.origin + (unsigned)ru +
-                                      (unsigned)rv * (unsigned)grid_size;
-                if (cell != cur[q])
-                {
-                    if (cur[q] != 0xffffffffu)
-                    {
-                        flush(grid, cur[q], cells, are[q], aim[q], status);
-                        ++flushes;
-                    }
-                    are[q] = aim[q] = GT(0);
-                    cur[q] = cell;
-                }
+                if (q >= rows_here) break;
+                const int b = b0 + q * lay.groups;
+                const unsigned rv = min((unsigned)(b + v.mv),
+                                        (unsigned)(b + v.mv - w));
+                const auto k = KernelLoad<KT>::get(
+                    slab[kbase + (int)rv * pitch]);
+                const unsigned cell = cell0 + rv * (unsigned)grid_size;
+                const bool change = cell != cur[q];
+                // cur = 0xffffffff (no cell yet) is >= cells: nothing to add.
+                red_add_c_if(change && cur[q] < cells,
+                             grid + 2 * (size_t)cur[q], are[q], aim[q]);
+                flushes += change;
+                are[q] = change ? GT(0) : are[q];
+                aim[q] = change ? GT(0) : aim[q];
+                cur[q] = cell;
                 are[q] = fma(v.ar, (GT)k.x, are[q]);
                 are[q] = fma(-v.ai, (GT)k.y, are[q]);
                 aim[q] = fma(v.bi, (GT)k.x, aim[q]);
@@ -160,11 +266,8 @@ __device__ __forceinline__ void process_task(const TapVis<GT>* __restrict__ s_vi
         }
 #pragma unroll
         for (int q = 0; q < CPT; ++q)
-            if (act[q] && cur[q] != 0xffffffffu)
-            {
-                flush(grid, cur[q], cells, are[q], aim[q], status);
-                ++flushes;
-            }
+            red_add_c_if(cur[q] < cells, grid + 2 * (size_t)cur[q], are[q],
+                         aim[q]);
     }
 }
 
@@ -179,6 +282,7 @@ romein_grid_kernel(const GridArgs a)
         smem + (STAGED ? a.slab_smem_bytes : 0));
     __shared__ uint64_t s_bar;
     __shared__ unsigned s_task;
+    __shared__ uint32_t s_order[kGridThreads];
 
     const V2* __restrict__ svis = static_cast<const V2*>(a.svis);
     const KT* __restrict__ slabs = static_cast<const KT*>(a.slabs);
@@ -227,9 +331,14 @@ romein_grid_kernel(const GridArgs a)
                 bulk_copy_g2s(smem + off, src + off,
                               min(kBulkChunk, d.bytes - off), &s_bar);
         }
-        for (int i = threadIdx.x; i < m; i += kGridThreads)
-            s_vis[i] = derive<GT>(a.srec[begin + i], svis[begin + i], d,
-                                  a.grid_size, a.oversample, a.half);
+        // Order the task's visibilities by (row offset, cell) so that each
+        // stretch of the task reads one row block of the slab (a fifth of it
+        // at oversample 4) and consecutive visibilities are neighbours.
+        const int src = task_order(a.srec, begin, m, s_order);
+        if (threadIdx.x < m)
+            s_vis[threadIdx.x] = derive<GT>(a.srec[begin + src],
+                                            svis[begin + src], d, a.grid_size,
+                                            a.oversample, a.half, status);
         if (load)
         {
             const bool ok = mbar_wait_bounded(&s_bar, phase);
@@ -250,16 +359,21 @@ romein_grid_kernel(const GridArgs a)
         }
         const KT* slab = STAGED ? s_slab : slabs + d.offset;
         const int w = 2 * d.support + 1;
-        const int cpt = d.support < kTuneMax ? a.cpt[d.support] : 4;
-        if (cpt == 1)
-            process_task<GT, KT, 1>(s_vis, m, w, d.pitch, slab, grid,
-                                    a.grid_size, cells, status, flushes);
-        else if (cpt == 2)
-            process_task<GT, KT, 2>(s_vis, m, w, d.pitch, slab, grid,
-                                    a.grid_size, cells, status, flushes);
-        else
-            process_task<GT, KT, 4>(s_vis, m, w, d.pitch, slab, grid,
-                                    a.grid_size, cells, status, flushes);
+        const int cpt = d.support < kTuneMax ? a.cpt[d.support] : 5;
+        switch (cpt)
+        {
+#define B200_CASE(C)                                                        \
+        case C:                                                             \
+            process_task<GT, KT, C>(s_vis, m, w, d.pitch, slab, grid,       \
+                                    a.grid_size, cells, flushes);           \
+            break;
+        B200_CASE(1) B200_CASE(2) B200_CASE(3) B200_CASE(4) B200_CASE(6)
+        B200_CASE(8)
+        default:
+            process_task<GT, KT, 5>(s_vis, m, w, d.pitch, slab, grid,
+                                    a.grid_size, cells, flushes);
+#undef B200_CASE
+        }
     }
     const unsigned long long f = warp_sum((unsigned long long)flushes);
     if ((threadIdx.x & 31) == 0 && f)
@@ -271,13 +385,35 @@ cudaError_t launch_variant(const GridArgs& a, int num_sms, size_t smem,
                            cudaStream_t st, int* ctas_out)
 {
     auto fn = romein_grid_kernel<GT, KT, STAGED>;
-    cudaError_t e = cudaFuncSetAttribute(
-        fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // Function attributes and occupancy are looked up once per (variant,
+    // device, shared-memory size), not on every launch.
+    static std::mutex mu;
+    static int cached_dev = -1;
+    static size_t cached_smem = 0;
+    static int cached_per_sm = 0;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn,
-                                                      kGridThreads, smem);
-    if (e != cudaSuccess) return e;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (dev == cached_dev && smem == cached_smem)
+        {
+            per_sm = cached_per_sm;
+        }
+        else
+        {
+            e = cudaFuncSetAttribute(
+                fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &per_sm, fn, kGridThreads, smem);
+            if (e != cudaSuccess) return e;
+            cached_dev = dev;
+            cached_smem = smem;
+            cached_per_sm = per_sm;
+        }
+    }
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     const int ctas = num_sms * per_sm;
     if (ctas_out) *ctas_out = ctas;
@@ -287,27 +423,42 @@ cudaError_t launch_variant(const GridArgs& a, int num_sms, size_t smem,
 
 }  // namespace
 
-// Classes-per-thread for each support: the choice that keeps the most
-// thread slots busy (W^2 classes over 256 threads, sliced over the task's
-// visibilities when W^2 is small), preferring more classes per thread on
-// ties for the extra independent work per tap record.
+// Rows-per-thread (CPT) for each support, from a cost model of
+// process_task: per visibility a thread does ~12 instructions of shared
+// column work plus ~20 per class, so the cost of a tap is
+// (12 / CPT + 20) / utilisation, utilisation being the fraction of the
+// CTA's thread slots holding a live class.
 void default_tune_table(unsigned char* cpt)
 {
+    const int choices[] = {1, 2, 3, 4, 5, 6, 8};
     for (int s = 0; s < kTuneMax; ++s)
     {
-        const int classes = (2 * s + 1) * (2 * s + 1);
-        double best = -1.0;
+        const int w = 2 * s + 1;
+        double best = 1e30;
         int pick = 1;
-        for (int c : {1, 2, 4})
+        for (int c : choices)
         {
-            const int tps = std::min(kGridThreads, (classes + c - 1) / c);
-            const int slices = kGridThreads / tps;
-            const int passes = (classes + tps * c - 1) / (tps * c);
-            const double util = (double)classes * slices /
-                                ((double)kGridThreads * c * passes);
-            if (util >= best - 1e-9)
+            const int need = (w + c - 1) / c;
+            int groups, passes, slices;
+            if (w * need <= kGridThreads)
             {
-                best = util;
+                groups = need;
+                passes = 1;
+                slices = kGridThreads / (w * need);
+            }
+            else
+            {
+                groups = kGridThreads / w;
+                passes = (w + groups * c - 1) / (groups * c);
+                slices = 1;
+            }
+            (void)groups;
+            const double util = (double)w * w * slices /
+                                ((double)kGridThreads * c * passes);
+            const double cost = (12.0 / c + 20.0) / util;
+            if (cost < best - 1e-9)
+            {
+                best = cost;
                 pick = c;
             }
         }

@@ -16,20 +16,24 @@ namespace b200 {
 //
 // The reference stores, per w-plane, the non-negative quadrant of the
 // oversampled kernel, indexed by |off + tap * oversample| in each axis
-// (oskar_grid_wproj.c:110-117).  A tap sequence tap = -S..S therefore walks
-// the quadrant with stride `oversample`.  Each plane is re-laid
-// "phase-major": quadrant index x goes to position (x % os) * L + x / os,
-// L = ceil(E / os), E = os * S + ceil(os / 2) + 1 (the entries the plane can
-// use).  Consecutive taps then read consecutive positions (one run for the
-// taps with off + tap * os >= 0 and one descending run for the rest), so a
-// warp's 32 kernel reads are contiguous in shared memory.
+// (oskar_grid_wproj.c:110-117).  Each plane becomes one "slab":
+//   columns: quadrant column x goes to position (x % os) * L + x / os,
+//     L = ceil(E / os), E = os * S + ceil(os / 2) + 1 (the entries the plane
+//     can use).  The taps k = -S..S of one visibility then read consecutive
+//     positions (an ascending run for off + k * os >= 0, a descending run
+//     for the rest), so a warp's kernel reads are contiguous.
+//   rows: expanded per row offset.  Row (off_v + H) * W + (j + S),
+//     W = 2S + 1, H = ceil(os / 2), holds quadrant row |off_v + j * os|.
+//     A visibility's tap rows j = -S..S are then W consecutive slab rows, so
+//     the row part of a tap's index is linear in the tap row.
 // ---------------------------------------------------------------------------
 struct PlaneDesc
 {
     int support;        // S
     int extent;         // E
-    int L;              // positions per oversample phase
+    int L;              // column positions per oversample phase
     int pitch;          // row length of the slab in elements (os * L)
+    int rows;           // slab rows: (2H + 1) * (2S + 1)
     long long offset;   // element offset of the slab in the slab array
     unsigned bytes;     // slab bytes, rounded up to 16
     float scale;        // stored value = true value / scale (1 unless F16/BF16)

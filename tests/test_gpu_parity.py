@@ -195,7 +195,7 @@ def _grid_ext(ws, w, single, **opt):
     real = np.float32 if single else np.float64
     tdt = torch.float32 if single else torch.float64
     cube = fg.Cube(ws, w["support"], w["oversample"], w["conv_size_half"],
-                   w["conv_func"], data_is_double=not single,
+                   np.asarray(w["conv_func"], real), data_is_double=not single,
                    kernel_type=opt.pop("kernel_type", _lib.KERNEL_NATIVE))
     g = w["grid_size"]
     grid = torch.zeros(2 * g * g, dtype=tdt, device="cuda")
