@@ -97,7 +97,8 @@ __global__ void relayout_kernel(const IN* __restrict__ cube,
         // x = (pos % L) * os + pos / L
         const int xu = (col % d.L) * oversample + col / d.L;
         double re = 0.0, im = 0.0;
-        if (xu < d.extent)
+        // Columns past os * L are padding.
+        if (col < oversample * d.L && xu < d.extent)
         {
             const long long f = base + (long long)xv * conv_size_half + xu;
             re = (double)cube[2 * f];
@@ -156,14 +157,20 @@ int cube_build(oskar_B200Cube* c, const void* d_conv, int conv_is_double,
     // Slab geometry and offsets (host).
     long long off = 0;
     unsigned max_bytes = 0;
+    c->max_block_bytes = 0;
     const size_t align_elems = 16 / c->elem_bytes > 0 ? 16 / c->elem_bytes : 1;
     for (int p = 0; p < P; ++p)
     {
         PlaneDesc& d = c->planes[p];
         d.extent = os * d.support + c->half + 1;
         d.L = (d.extent + os - 1) / os;
-        d.pitch = os * d.L;
+        // Rows padded to 4 elements: every W-row block is then a multiple
+        // of 16 bytes and starts 16-byte aligned (bulk-copy rules).
+        d.pitch = (os * d.L + 3) / 4 * 4;
         d.rows = (2 * c->half + 1) * (2 * d.support + 1);
+        const unsigned block = (unsigned)((2 * d.support + 1) * d.pitch *
+                                          c->elem_bytes);
+        if (block > c->max_block_bytes) c->max_block_bytes = block;
         d.offset = off;
         const size_t elems = (size_t)d.rows * d.pitch;
         const size_t padded = (elems + align_elems - 1) / align_elems *

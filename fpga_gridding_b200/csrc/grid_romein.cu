@@ -102,12 +102,13 @@ __device__ __forceinline__ uint32_t spread9(uint32_t x)
     return x;
 }
 
-// Returns, for thread t < m, the task-relative index of the t-th
-// visibility in (row offset, Morton cell) order.  Bitonic sort of one key
+// Returns, for thread t < m, the sort key of the t-th visibility in
+// (row offset, Morton cell) order; its low 8 bits are the task-relative
+// index of that visibility and bits 26-31 its row offset + half.  Bitonic sort of one key
 // per thread: key = (off_v + half) << 26 | Morton(gu, gv low 9 bits) << 8 |
 // index (m <= 256, half <= 16); strides below 32 use warp shuffles, larger
 // ones go through shared memory.  All threads of the CTA must call it.
-__device__ __forceinline__ int task_order(const int4* __restrict__ srec,
+__device__ __forceinline__ uint32_t task_order(const int4* __restrict__ srec,
                                           uint32_t begin, int m,
                                           uint32_t* s_order)
 {
@@ -144,7 +145,7 @@ __device__ __forceinline__ int task_order(const int4* __restrict__ srec,
             key = take_min ? min(key, other) : max(key, other);
         }
     }
-    return (int)(key & 0xffu);
+    return key;
 }
 
 // Predicated complex flush: one vector reduction when `pred` holds, no
@@ -204,6 +205,7 @@ __device__ __forceinline__ TaskLayout task_layout(int w)
 template <typename GT, typename KT, int CPT>
 __device__ __forceinline__ void process_task(const TapVis<GT>* __restrict__ s_vis,
                                              int m, int w, int pitch,
+                                             int row_shift,
                                              const KT* __restrict__ slab,
                                              GT* __restrict__ grid,
                                              int grid_size, unsigned cells,
@@ -238,7 +240,7 @@ __device__ __forceinline__ void process_task(const TapVis<GT>* __restrict__ s_vi
             const unsigned ru = min((unsigned)(a + v.mu),
                                     (unsigned)(a + v.mu - w));
             const int col = (int)ru >= v.tu ? v.cp + (int)ru : v.cn - (int)ru;
-            const int kbase = v.rowbase + col;
+            const int kbase = v.rowbase - row_shift + col;
             const unsigned cell0 = v.origin + ru;
 #pragma unroll
             for (int q = 0; q < CPT; ++q)
@@ -271,18 +273,50 @@ __device__ __forceinline__ void process_task(const TapVis<GT>* __restrict__ s_vi
     }
 }
 
+template <typename GT, typename KT, int CPT>
+__device__ __forceinline__ void run_cpt(const TapVis<GT>* s_vis, int m, int w,
+                                        int pitch, int row_shift,
+                                        const KT* slab, GT* grid,
+                                        int grid_size, unsigned cells,
+                                        unsigned& flushes)
+{
+    process_task<GT, KT, CPT>(s_vis, m, w, pitch, row_shift, slab, grid,
+                              grid_size, cells, flushes);
+}
+
+template <typename GT, typename KT>
+__device__ __forceinline__ void dispatch_cpt(int cpt, const TapVis<GT>* s_vis,
+                                             int m, int w, int pitch,
+                                             int row_shift, const KT* slab,
+                                             GT* grid, int grid_size,
+                                             unsigned cells, unsigned& flushes)
+{
+    switch (cpt)
+    {
+    case 1: run_cpt<GT, KT, 1>(s_vis, m, w, pitch, row_shift, slab, grid, grid_size, cells, flushes); break;
+    case 2: run_cpt<GT, KT, 2>(s_vis, m, w, pitch, row_shift, slab, grid, grid_size, cells, flushes); break;
+    case 3: run_cpt<GT, KT, 3>(s_vis, m, w, pitch, row_shift, slab, grid, grid_size, cells, flushes); break;
+    case 4: run_cpt<GT, KT, 4>(s_vis, m, w, pitch, row_shift, slab, grid, grid_size, cells, flushes); break;
+    case 6: run_cpt<GT, KT, 6>(s_vis, m, w, pitch, row_shift, slab, grid, grid_size, cells, flushes); break;
+    case 8: run_cpt<GT, KT, 8>(s_vis, m, w, pitch, row_shift, slab, grid, grid_size, cells, flushes); break;
+    default: run_cpt<GT, KT, 5>(s_vis, m, w, pitch, row_shift, slab, grid, grid_size, cells, flushes); break;
+    }
+}
+
 template <typename GT, typename KT, bool STAGED>
 __global__ void __launch_bounds__(kGridThreads)
 romein_grid_kernel(const GridArgs a)
 {
     using V2 = typename Vec2<GT>::type;
     extern __shared__ __align__(128) unsigned char smem[];
-    KT* s_slab = reinterpret_cast<KT*>(smem);
+    // STAGED: [row block of the current run][tap records]; else [records]
+    KT* s_block = reinterpret_cast<KT*>(smem);
     TapVis<GT>* s_vis = reinterpret_cast<TapVis<GT>*>(
-        smem + (STAGED ? a.slab_smem_bytes : 0));
+        smem + (STAGED ? a.block_smem_bytes : 0));
     __shared__ uint64_t s_bar;
     __shared__ unsigned s_task;
     __shared__ uint32_t s_order[kGridThreads];
+    __shared__ int s_run_begin[kMaxOffsets], s_run_end[kMaxOffsets];
 
     const V2* __restrict__ svis = static_cast<const V2*>(a.svis);
     const KT* __restrict__ slabs = static_cast<const KT*>(a.slabs);
@@ -290,6 +324,7 @@ romein_grid_kernel(const GridArgs a)
     unsigned long long* status = &a.counters[CNT_STATUS];
     const unsigned num_tasks = (unsigned)a.counters[CNT_TASKS];
     const unsigned cells = (unsigned)a.grid_size * (unsigned)a.grid_size;
+    const int offsets = 2 * a.half + 1;
 
     if (STAGED && threadIdx.x == 0)
     {
@@ -299,14 +334,18 @@ romein_grid_kernel(const GridArgs a)
     __syncthreads();
 
     uint32_t phase = 0;
-    int cur_plane = -1;
     unsigned flushes = 0;
     for (;;)
     {
         if (threadIdx.x == 0)
             s_task = (unsigned)atomicAdd(&a.counters[CNT_TASK_NEXT], 1ull);
+        if (threadIdx.x < offsets)
+        {
+            s_run_begin[threadIdx.x] = 0;
+            s_run_end[threadIdx.x] = 0;
+        }
         // Also: every thread has finished with the previous task's records
-        // and slab before they are overwritten below.
+        // and row block before they are overwritten below.
         __syncthreads();
         const unsigned task = s_task;
         if (task >= num_tasks) break;
@@ -320,27 +359,58 @@ romein_grid_kernel(const GridArgs a)
         }
         const int plane = a.srec[begin].z & 0x7fffffff;
         const PlaneDesc d = a.planes[plane];
-        const bool load = STAGED && plane != cur_plane;
-        if (load && threadIdx.x == 0)
+        const int w = 2 * d.support + 1;
+        const int cpt = d.support < kTuneMax ? a.cpt[d.support] : 5;
+
+        // Order the task's visibilities by (row offset, cell): each run of
+        // one row offset reads one W-row block of the plane's slab, and
+        // consecutive visibilities are neighbours.
+        const uint32_t key = task_order(a.srec, begin, m, s_order);
+        const int t = threadIdx.x;
+        if (t < m)
         {
-            fence_proxy_async_shared();
-            mbar_arrive_expect_tx(&s_bar, d.bytes);
-            const unsigned char* src =
-                reinterpret_cast<const unsigned char*>(slabs + d.offset);
-            for (unsigned off = 0; off < d.bytes; off += kBulkChunk)
-                bulk_copy_g2s(smem + off, src + off,
-                              min(kBulkChunk, d.bytes - off), &s_bar);
+            const int src = (int)(key & 0xffu);
+            s_vis[t] = derive<GT>(a.srec[begin + src], svis[begin + src], d,
+                                  a.grid_size, a.oversample, a.half, status);
+            s_order[t] = key;
         }
-        // Order the task's visibilities by (row offset, cell) so that each
-        // stretch of the task reads one row block of the slab (a fifth of it
-        // at oversample 4) and consecutive visibilities are neighbours.
-        const int src = task_order(a.srec, begin, m, s_order);
-        if (threadIdx.x < m)
-            s_vis[threadIdx.x] = derive<GT>(a.srec[begin + src],
-                                            svis[begin + src], d, a.grid_size,
-                                            a.oversample, a.half, status);
-        if (load)
+        __syncthreads();
+        if (t < m)
         {
+            const int ov = (int)(key >> 26);
+            if (t == 0 || (int)(s_order[t - 1] >> 26) != ov)
+                s_run_begin[ov] = t;
+            if (t == m - 1 || (int)(s_order[t + 1] >> 26) != ov)
+                s_run_end[ov] = t + 1;
+        }
+        __syncthreads();
+
+        if (!STAGED)
+        {
+            dispatch_cpt<GT, KT>(cpt, s_vis, m, w, d.pitch, 0,
+                                 slabs + d.offset, grid, a.grid_size, cells,
+                                 flushes);
+            continue;
+        }
+        const unsigned block_elems = (unsigned)w * (unsigned)d.pitch;
+        const unsigned block_bytes = block_elems * (unsigned)sizeof(KT);
+        for (int ov = 0; ov < offsets; ++ov)
+        {
+            const int rb = s_run_begin[ov], re = s_run_end[ov];
+            if (re <= rb) continue;
+            if (threadIdx.x == 0)
+            {
+                // Every thread finished reading the previous block (barrier
+                // below / above); order that before the async-proxy write.
+                fence_proxy_async_shared();
+                mbar_arrive_expect_tx(&s_bar, block_bytes);
+                const unsigned char* src = reinterpret_cast<const unsigned char*>(
+                    slabs + d.offset + (long long)ov * block_elems);
+                for (unsigned off = 0; off < block_bytes; off += kBulkChunk)
+                    bulk_copy_g2s(reinterpret_cast<unsigned char*>(s_block) + off,
+                                  src + off, min(kBulkChunk, block_bytes - off),
+                                  &s_bar);
+            }
             const bool ok = mbar_wait_bounded(&s_bar, phase);
             if (!__syncthreads_and(ok))
             {
@@ -351,28 +421,10 @@ romein_grid_kernel(const GridArgs a)
                 return;
             }
             phase ^= 1u;
-            cur_plane = plane;
-        }
-        else
-        {
+            dispatch_cpt<GT, KT>(cpt, s_vis + rb, re - rb, w, d.pitch,
+                                 ov * (int)block_elems, s_block, grid,
+                                 a.grid_size, cells, flushes);
             __syncthreads();
-        }
-        const KT* slab = STAGED ? s_slab : slabs + d.offset;
-        const int w = 2 * d.support + 1;
-        const int cpt = d.support < kTuneMax ? a.cpt[d.support] : 5;
-        switch (cpt)
-        {
-#define B200_CASE(C)                                                        \
-        case C:                                                             \
-            process_task<GT, KT, C>(s_vis, m, w, d.pitch, slab, grid,       \
-                                    a.grid_size, cells, flushes);           \
-            break;
-        B200_CASE(1) B200_CASE(2) B200_CASE(3) B200_CASE(4) B200_CASE(6)
-        B200_CASE(8)
-        default:
-            process_task<GT, KT, 5>(s_vis, m, w, d.pitch, slab, grid,
-                                    a.grid_size, cells, flushes);
-#undef B200_CASE
         }
     }
     const unsigned long long f = warp_sum((unsigned long long)flushes);
@@ -470,8 +522,8 @@ size_t grid_smem_bytes(const oskar_B200Cube* cube, bool staged)
 {
     const size_t rec = cube->data_is_double ? sizeof(TapVis<double>)
                                             : sizeof(TapVis<float>);
-    const size_t slab = staged ? ((cube->max_slab_bytes + 127) / 128) * 128 : 0;
-    return slab + rec * kTaskMax;
+    const size_t block = staged ? ((cube->max_block_bytes + 127) / 128) * 128 : 0;
+    return block + rec * kTaskMax;
 }
 
 cudaError_t launch_grid(const GridArgs& a, const oskar_B200Cube* cube,
@@ -480,9 +532,9 @@ cudaError_t launch_grid(const GridArgs& a, const oskar_B200Cube* cube,
 {
     const size_t smem = grid_smem_bytes(cube, staged);
     GridArgs args = a;
-    args.slab_smem_bytes = staged ? (unsigned)(((cube->max_slab_bytes + 127) /
-                                                128) * 128)
-                                  : 0u;
+    args.block_smem_bytes = staged ? (unsigned)(((cube->max_block_bytes + 127) /
+                                                  128) * 128)
+                                    : 0u;
     if (cube->data_is_double)
     {
         if (cube->kernel_type != OSKAR_B200_KERNEL_NATIVE)

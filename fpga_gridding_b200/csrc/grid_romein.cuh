@@ -9,6 +9,7 @@ constexpr int kGridThreads = 256;   // threads per CTA
 constexpr int kTaskMax = 256;       // visibilities per task
 constexpr int kTuneMax = 128;       // supports covered by the tune table
 constexpr unsigned kBulkChunk = 32768;  // bytes per cp.async.bulk
+constexpr int kMaxOffsets = 33;     // 2 * ceil(oversample / 2) + 1, oversample <= 32
 
 struct GridArgs
 {
@@ -22,7 +23,7 @@ struct GridArgs
     int grid_size;
     int oversample;
     int half;
-    unsigned slab_smem_bytes;   // set by launch_grid
+    unsigned block_smem_bytes;  // set by launch_grid
     unsigned char cpt[kTuneMax];
 };
 

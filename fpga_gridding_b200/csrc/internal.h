@@ -98,6 +98,7 @@ struct oskar_B200Cube
     int kernel_type = OSKAR_B200_KERNEL_NATIVE;
     int elem_bytes = 0;      // bytes per stored complex value
     unsigned max_slab_bytes = 0;
+    unsigned max_block_bytes = 0;   // largest W-row block (one row offset)
     int max_support = 0;
     std::vector<b200::PlaneDesc> planes;
     b200::DeviceBuffer d_planes, d_slabs, d_norm_table, d_support;
