@@ -80,12 +80,8 @@ def barrier(world):
 
 
 def max_over_ranks(x, world):
-    if world == 1:
-        return x
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from fpga_gridding_b200 import replicas
+    return replicas.max_over_ranks(x, world, device="cuda")
 
 
 def measured_peaks():

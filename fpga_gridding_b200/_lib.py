@@ -24,7 +24,6 @@ EXPORTED_SYMBOLS = (
     "oskar_b200_cube_free",
     "oskar_b200_cube_bytes",
     "oskar_b200_grid",
-    "oskar_b200_fold_compensation",
     "oskar_b200_place",
     "oskar_b200_last_stats",
     "oskar_b200_set_stage_timing",
@@ -108,7 +107,6 @@ def load():
     lib.oskar_b200_grid.argtypes = [
         _P, _P, C.POINTER(Options), _SZ, _P, _P, _P, _P, _P, C.c_double,
         C.c_double, C.c_int, _P, _P, _P, _P]
-    lib.oskar_b200_fold_compensation.argtypes = [_P, _P, C.c_int, _P]
     lib.oskar_b200_place.argtypes = [
         _P, C.c_int, C.c_int, _SZ, _P, C.c_int, _SZ, _P, _P, _P, C.c_double,
         C.c_double, C.c_int] + [_P] * 7 + [_P]
@@ -119,7 +117,7 @@ def load():
         _P, _P, C.c_int, C.c_int, C.POINTER(C.c_double)]
     for name in ("oskar_b200_workspace_create", "oskar_b200_workspace_free",
                  "oskar_b200_cube_create", "oskar_b200_cube_free",
-                 "oskar_b200_grid", "oskar_b200_fold_compensation",
+                 "oskar_b200_grid",
                  "oskar_b200_place", "oskar_b200_last_stats",
                  "oskar_b200_set_stage_timing",
                  "oskar_b200_measure_atomic_rate"):

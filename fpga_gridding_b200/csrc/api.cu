@@ -194,7 +194,11 @@ int check_options(const oskar_B200Options* opt, int data_is_double)
         return OSKAR_B200_ERR_INVALID_ARGUMENT;
     if (data_is_double && opt->coord_mode != OSKAR_B200_COORDS_F64)
         return OSKAR_B200_ERR_UNSUPPORTED;
-    if (opt->accum_mode != OSKAR_B200_ACCUM_PLAIN)
+    if (opt->accum_mode != OSKAR_B200_ACCUM_PLAIN &&
+        opt->accum_mode != OSKAR_B200_ACCUM_COMPENSATED)
+        return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    if (opt->accum_mode == OSKAR_B200_ACCUM_COMPENSATED &&
+        (data_is_double || opt->staging == 1))
         return OSKAR_B200_ERR_UNSUPPORTED;
     if (opt->staging < 0 || opt->staging > 2)
         return OSKAR_B200_ERR_INVALID_ARGUMENT;
@@ -508,13 +512,6 @@ int oskar_b200_grid(oskar_B200Workspace* ws, const oskar_B200Cube* cube,
     return run_grid(ws, cube, opt, num_points, uu, vv, ww, vis, weight,
                     cell_size_rad, w_scale, grid_size, grid, d_num_skipped,
                     d_norm, s);
-}
-
-int oskar_b200_fold_compensation(oskar_B200Workspace* ws, void* grid,
-                                 int grid_size, void* stream)
-{
-    (void)ws; (void)grid; (void)grid_size; (void)stream;
-    return OSKAR_B200_ERR_UNSUPPORTED;
 }
 
 int oskar_b200_place(oskar_B200Workspace* ws, int data_is_double,

@@ -201,13 +201,55 @@ __device__ __forceinline__ TaskLayout task_layout(int w)
     return t;
 }
 
+// Grid flush policies.  PlainFlush: one predicated vector reduction.
+// CompensatedFlush (FP32): the addition returns the old value; Knuth's
+// TwoSum recovers the exact rounding error of old + x (the atomic rounds to
+// nearest even), which is added to a compensation grid folded into the grid
+// at the end of the job.  Its branch is taken only when the lane flushes.
+template <typename GT>
+struct PlainFlush
+{
+    GT* grid;
+    __device__ __forceinline__ void operator()(bool pred, unsigned cell, GT re,
+                                               GT im) const
+    {
+        red_add_c_if(pred, grid + 2 * (size_t)cell, re, im);
+    }
+};
+
+__device__ __forceinline__ float two_sum_err(float a, float b)
+{
+    const float s = __fadd_rn(a, b);
+    const float bb = __fsub_rn(s, a);
+    return __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+}
+
+struct CompensatedFlush
+{
+    float* grid;
+    float* comp;
+    __device__ __forceinline__ void operator()(bool pred, unsigned cell,
+                                               float re, float im) const
+    {
+        if (!pred) return;
+        float ore, oim;
+        asm volatile("atom.relaxed.gpu.global.add.v2.f32 {%0, %1}, [%2], {%3, %4};"
+                     : "=f"(ore), "=f"(oim)
+                     : "l"(grid + 2 * (size_t)cell), "f"(re), "f"(im)
+                     : "memory");
+        const float er = two_sum_err(ore, re), ei = two_sum_err(oim, im);
+        if (er != 0.f || ei != 0.f)
+            red_add_c(comp + 2 * (size_t)cell, er, ei);
+    }
+};
+
 // One task: every class of the W x W footprint over the task's visibilities.
-template <typename GT, typename KT, int CPT>
+template <typename GT, typename KT, int CPT, typename FL>
 __device__ __forceinline__ void process_task(const TapVis<GT>* __restrict__ s_vis,
                                              int m, int w, int pitch,
                                              int row_shift,
                                              const KT* __restrict__ slab,
-                                             GT* __restrict__ grid,
+                                             const FL& flush,
                                              int grid_size, unsigned cells,
                                              unsigned& flushes)
 {
@@ -254,8 +296,7 @@ __device__ __forceinline__ void process_task(const TapVis<GT>* __restrict__ s_vi
                 const unsigned cell = cell0 + rv * (unsigned)grid_size;
                 const bool change = cell != cur[q];
                 // cur = 0xffffffff (no cell yet) is >= cells: nothing to add.
-                red_add_c_if(change && cur[q] < cells,
-                             grid + 2 * (size_t)cur[q], are[q], aim[q]);
+                flush(change && cur[q] < cells, cur[q], are[q], aim[q]);
                 flushes += change;
                 are[q] = change ? GT(0) : are[q];
                 aim[q] = change ? GT(0) : aim[q];
@@ -268,42 +309,56 @@ __device__ __forceinline__ void process_task(const TapVis<GT>* __restrict__ s_vi
         }
 #pragma unroll
         for (int q = 0; q < CPT; ++q)
-            red_add_c_if(cur[q] < cells, grid + 2 * (size_t)cur[q], are[q],
-                         aim[q]);
+            flush(cur[q] < cells, cur[q], are[q], aim[q]);
     }
 }
 
-template <typename GT, typename KT, int CPT>
-__device__ __forceinline__ void run_cpt(const TapVis<GT>* s_vis, int m, int w,
-                                        int pitch, int row_shift,
-                                        const KT* slab, GT* grid,
-                                        int grid_size, unsigned cells,
-                                        unsigned& flushes)
-{
-    process_task<GT, KT, CPT>(s_vis, m, w, pitch, row_shift, slab, grid,
-                              grid_size, cells, flushes);
-}
-
-template <typename GT, typename KT>
+template <typename GT, typename KT, typename FL>
 __device__ __forceinline__ void dispatch_cpt(int cpt, const TapVis<GT>* s_vis,
                                              int m, int w, int pitch,
                                              int row_shift, const KT* slab,
-                                             GT* grid, int grid_size,
+                                             const FL& fl, int grid_size,
                                              unsigned cells, unsigned& flushes)
 {
+#define B200_CPT(C)                                                         \
+    process_task<GT, KT, C, FL>(s_vis, m, w, pitch, row_shift, slab, fl,    \
+                                grid_size, cells, flushes)
     switch (cpt)
     {
-    case 1: run_cpt<GT, KT, 1>(s_vis, m, w, pitch, row_shift, slab, grid, grid_size, cells, flushes); break;
-    case 2: run_cpt<GT, KT, 2>(s_vis, m, w, pitch, row_shift, slab, grid, grid_size, cells, flushes); break;
-    case 3: run_cpt<GT, KT, 3>(s_vis, m, w, pitch, row_shift, slab, grid, grid_size, cells, flushes); break;
-    case 4: run_cpt<GT, KT, 4>(s_vis, m, w, pitch, row_shift, slab, grid, grid_size, cells, flushes); break;
-    case 6: run_cpt<GT, KT, 6>(s_vis, m, w, pitch, row_shift, slab, grid, grid_size, cells, flushes); break;
-    case 8: run_cpt<GT, KT, 8>(s_vis, m, w, pitch, row_shift, slab, grid, grid_size, cells, flushes); break;
-    default: run_cpt<GT, KT, 5>(s_vis, m, w, pitch, row_shift, slab, grid, grid_size, cells, flushes); break;
+    case 1: B200_CPT(1); break;
+    case 2: B200_CPT(2); break;
+    case 3: B200_CPT(3); break;
+    case 4: B200_CPT(4); break;
+    case 6: B200_CPT(6); break;
+    case 8: B200_CPT(8); break;
+    default: B200_CPT(5); break;
     }
+#undef B200_CPT
 }
 
-template <typename GT, typename KT, bool STAGED>
+template <typename GT, bool COMP> struct FlushFor { using type = PlainFlush<GT>; };
+template <> struct FlushFor<float, true> { using type = CompensatedFlush; };
+
+template <typename GT, bool COMP>
+__device__ __forceinline__ typename FlushFor<GT, COMP>::type
+make_flush(void* grid, void* comp);
+template <>
+__device__ __forceinline__ PlainFlush<float> make_flush<float, false>(void* grid, void*)
+{
+    return PlainFlush<float>{static_cast<float*>(grid)};
+}
+template <>
+__device__ __forceinline__ PlainFlush<double> make_flush<double, false>(void* grid, void*)
+{
+    return PlainFlush<double>{static_cast<double*>(grid)};
+}
+template <>
+__device__ __forceinline__ CompensatedFlush make_flush<float, true>(void* grid, void* comp)
+{
+    return CompensatedFlush{static_cast<float*>(grid), static_cast<float*>(comp)};
+}
+
+template <typename GT, typename KT, bool STAGED, bool COMP>
 __global__ void __launch_bounds__(kGridThreads)
 romein_grid_kernel(const GridArgs a)
 {
@@ -320,7 +375,7 @@ romein_grid_kernel(const GridArgs a)
 
     const V2* __restrict__ svis = static_cast<const V2*>(a.svis);
     const KT* __restrict__ slabs = static_cast<const KT*>(a.slabs);
-    GT* __restrict__ grid = static_cast<GT*>(a.grid);
+    const auto fl = make_flush<GT, COMP>(a.grid, a.comp);
     unsigned long long* status = &a.counters[CNT_STATUS];
     const unsigned num_tasks = (unsigned)a.counters[CNT_TASKS];
     const unsigned cells = (unsigned)a.grid_size * (unsigned)a.grid_size;
@@ -388,7 +443,7 @@ romein_grid_kernel(const GridArgs a)
         if (!STAGED)
         {
             dispatch_cpt<GT, KT>(cpt, s_vis, m, w, d.pitch, 0,
-                                 slabs + d.offset, grid, a.grid_size, cells,
+                                 slabs + d.offset, fl, a.grid_size, cells,
                                  flushes);
             continue;
         }
@@ -422,7 +477,7 @@ romein_grid_kernel(const GridArgs a)
             }
             phase ^= 1u;
             dispatch_cpt<GT, KT>(cpt, s_vis + rb, re - rb, w, d.pitch,
-                                 ov * (int)block_elems, s_block, grid,
+                                 ov * (int)block_elems, s_block, fl,
                                  a.grid_size, cells, flushes);
             __syncthreads();
         }
@@ -432,11 +487,11 @@ romein_grid_kernel(const GridArgs a)
         atomicAdd(&a.counters[CNT_FLUSHES], f);
 }
 
-template <typename GT, typename KT, bool STAGED>
+template <typename GT, typename KT, bool STAGED, bool COMP = false>
 cudaError_t launch_variant(const GridArgs& a, int num_sms, size_t smem,
                            cudaStream_t st, int* ctas_out)
 {
-    auto fn = romein_grid_kernel<GT, KT, STAGED>;
+    auto fn = romein_grid_kernel<GT, KT, STAGED, COMP>;
     // Function attributes and occupancy are looked up once per (variant,
     // device, shared-memory size), not on every launch.
     static std::mutex mu;
@@ -518,6 +573,37 @@ void default_tune_table(unsigned char* cpt)
     }
 }
 
+namespace {
+
+__global__ void fold_kernel(float2* __restrict__ grid, float2* __restrict__ comp,
+                            size_t cells)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < cells;
+         i += (size_t)gridDim.x * blockDim.x)
+    {
+        const float2 c = comp[i];
+        if (c.x != 0.f || c.y != 0.f)
+        {
+            float2 g = grid[i];
+            g.x += c.x;
+            g.y += c.y;
+            grid[i] = g;
+            comp[i] = make_float2(0.f, 0.f);
+        }
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_fold(float* grid, float* comp, size_t cells, int num_sms,
+                        cudaStream_t st)
+{
+    fold_kernel<<<num_sms * 8, 256, 0, st>>>(reinterpret_cast<float2*>(grid),
+                                            reinterpret_cast<float2*>(comp),
+                                            cells);
+    return cudaGetLastError();
+}
+
 size_t grid_smem_bytes(const oskar_B200Cube* cube, bool staged)
 {
     const size_t rec = cube->data_is_double ? sizeof(TapVis<double>)
@@ -527,14 +613,29 @@ size_t grid_smem_bytes(const oskar_B200Cube* cube, bool staged)
 }
 
 cudaError_t launch_grid(const GridArgs& a, const oskar_B200Cube* cube,
-                        bool staged, int num_sms, cudaStream_t st,
-                        int* ctas_out)
+                        bool staged, bool compensated, int num_sms,
+                        cudaStream_t st, int* ctas_out)
 {
     const size_t smem = grid_smem_bytes(cube, staged);
     GridArgs args = a;
     args.block_smem_bytes = staged ? (unsigned)(((cube->max_block_bytes + 127) /
                                                   128) * 128)
                                     : 0u;
+    if (compensated)
+    {
+        // FP32 grids only; kernel values read through L1.
+        if (cube->data_is_double || staged || !a.comp)
+            return cudaErrorInvalidValue;
+        switch (cube->kernel_type)
+        {
+        case OSKAR_B200_KERNEL_F16:
+            return launch_variant<float, __half2, false, true>(args, num_sms, smem, st, ctas_out);
+        case OSKAR_B200_KERNEL_BF16:
+            return launch_variant<float, __nv_bfloat162, false, true>(args, num_sms, smem, st, ctas_out);
+        default:
+            return launch_variant<float, float2, false, true>(args, num_sms, smem, st, ctas_out);
+        }
+    }
     if (cube->data_is_double)
     {
         if (cube->kernel_type != OSKAR_B200_KERNEL_NATIVE)

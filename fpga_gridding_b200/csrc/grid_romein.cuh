@@ -19,6 +19,7 @@ struct GridArgs
     const PlaneDesc* planes;
     const void* slabs;
     void* grid;
+    void* comp;                 // compensation grid (ACCUM_COMPENSATED) or null
     unsigned long long* counters;
     int grid_size;
     int oversample;
@@ -30,7 +31,10 @@ struct GridArgs
 void default_tune_table(unsigned char* cpt);
 size_t grid_smem_bytes(const oskar_B200Cube* cube, bool staged);
 cudaError_t launch_grid(const GridArgs& a, const oskar_B200Cube* cube,
-                        bool staged, int num_sms, cudaStream_t st,
-                        int* ctas_out);
+                        bool staged, bool compensated, int num_sms,
+                        cudaStream_t st, int* ctas_out);
+// grid[i] += comp[i]; comp[i] = 0 over 2 * cells floats.
+cudaError_t launch_fold(float* grid, float* comp, size_t cells,
+                        int num_sms, cudaStream_t st);
 
 }  // namespace b200

@@ -74,9 +74,8 @@ struct oskar_B200Workspace
     // drop-in staging of the caller's host arrays
     b200::DeviceBuffer in_uu, in_vv, in_ww, in_vis, in_weight, in_grid,
         in_cube, in_norm;
-    // compensation grid of ACCUM_COMPENSATED
+    // error grid of ACCUM_COMPENSATED
     b200::DeviceBuffer comp_grid;
-    size_t comp_cells = 0;
     // pinned host mirror of the device counters (stats)
     void* h_counters = nullptr;
     unsigned long long last_points = 0;
@@ -160,9 +159,6 @@ int run_place(oskar_B200Workspace* ws, int data_is_double, int coord_mode,
               int grid_size, int32_t* gu, int32_t* gv, int32_t* plane,
               int32_t* off_u, int32_t* off_v, int32_t* conj,
               int32_t* skipped, cudaStream_t st);
-
-int fold_compensation(oskar_B200Workspace* ws, void* grid, int grid_size,
-                      cudaStream_t st);
 
 int measure_atomic_rate(oskar_B200Workspace* ws, void* grid, int grid_size,
                         int iters, double* updates_per_s);

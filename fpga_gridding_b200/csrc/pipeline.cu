@@ -194,10 +194,27 @@ int run_grid(oskar_B200Workspace* ws, const oskar_B200Cube* cube,
     const bool fits = grid_smem_bytes(cube, true) <= ws->smem_optin;
     const bool staged = opt->staging == 1;
     if (staged && !fits) return OSKAR_B200_ERR_UNSUPPORTED;
+    const bool comp = opt->accum_mode == OSKAR_B200_ACCUM_COMPENSATED;
+    const size_t cells = (size_t)grid_size * (size_t)grid_size;
+    if (comp)
+    {
+        // Error grid of this job: zeroed here, folded into the grid below.
+        B200_TRY(ws->comp_grid.ensure(cells * 2 * sizeof(float)));
+        B200_TRY(cudaMemsetAsync(ws->comp_grid.ptr, 0,
+                                 cells * 2 * sizeof(float), st));
+        ga.comp = ws->comp_grid.ptr;
+    }
     int ctas = 0;
     B200_TRY(mark(3));
-    B200_TRY(launch_grid(ga, cube, staged, ws->num_sms, st, &ctas));
+    B200_TRY(launch_grid(ga, cube, staged, comp, ws->num_sms, st, &ctas));
     launches += 1;
+    if (comp)
+    {
+        B200_TRY(launch_fold(static_cast<float*>(grid),
+                             static_cast<float*>(ws->comp_grid.ptr), cells,
+                             ws->num_sms, st));
+        launches += 1;
+    }
     B200_TRY(mark(4));
     ws->events_recorded = timing ? 1 : 0;
     ws->last_launches = launches;

@@ -132,11 +132,14 @@ enum
     OSKAR_B200_KERNEL_BF16 = 2     /* BF16 with a per-plane scale */
 };
 
-/* Grid accumulation for FP32 data. */
+/* Grid accumulation for FP32 data.  COMPENSATED: every grid atomic returns
+ * the old value, the exact rounding error of the addition (TwoSum) goes to
+ * an FP32 error grid in the workspace (grid_size^2 complex), and the error
+ * grid is added into the grid at the end of the call. */
 enum
 {
     OSKAR_B200_ACCUM_PLAIN = 0,        /* FP32 register sums, FP32 atomics */
-    OSKAR_B200_ACCUM_COMPENSATED = 1   /* FP32 grid plus an FP32 error grid */
+    OSKAR_B200_ACCUM_COMPENSATED = 1   /* plus the compensated grid atomics */
 };
 
 typedef struct oskar_B200Options
@@ -195,11 +198,6 @@ OSKAR_B200_EXPORT int oskar_b200_grid(oskar_B200Workspace* ws,
         const void* vis, const void* weight, double cell_size_rad,
         double w_scale, int grid_size, void* grid,
         unsigned long long* d_num_skipped, double* d_norm, void* stream);
-
-/* The compensation (error) grid used by OSKAR_B200_ACCUM_COMPENSATED lives
- * in the workspace; this adds it into `grid` (FP32, device) and clears it. */
-OSKAR_B200_EXPORT int oskar_b200_fold_compensation(oskar_B200Workspace* ws,
-        void* grid, int grid_size, void* stream);
 
 /* Per-visibility placement exactly as the gridder computes it (device
  * pointers, int32 outputs, any may be NULL): grid cell, clamped w-plane,

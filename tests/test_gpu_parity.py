@@ -229,6 +229,22 @@ def test_stats_count_grid_updates(ws, oracle, small):
     assert 0 < st.atomic_flushes < st.grid_updates
 
 
+def test_compensated_accumulation(ws, oracle, small):
+    """The compensated grid atomics capture the rounding of every grid
+    addition: the result is at least as close to the FP64 oracle as the
+    plain FP32 one (plain_small piles 241,920 visibilities onto ~80^2
+    cells), and within the FP32 bar."""
+    _, n1, g1 = oracle.grid_d(promote(small), threads=8)
+    _, _, gp, _ = _grid_ext(ws, small, True)
+    s, n, gc, st = _grid_ext(ws, small, True,
+                             accum_mode=_lib.ACCUM_COMPENSATED)
+    ep, ec = oracle.rel_rms(gp, g1), oracle.rel_rms(gc, g1)
+    print(f"plain {ep:.3e} compensated {ec:.3e}")
+    assert st.status == 0 and s == 0
+    assert ec <= TOL_F and ec <= ep
+    assert abs(n - n1) <= TOL_D * abs(n1)
+
+
 @pytest.mark.parametrize("kt,tol", [(_lib.KERNEL_F16, 2e-3),
                                     (_lib.KERNEL_BF16, 2e-2)])
 def test_reduced_precision_kernels(ws, oracle, small, kt, tol):
