@@ -437,6 +437,320 @@ def audit_error(wl, m=200000):
                       "vs FP64 oracle on the same inputs"}
 
 
+BATCH_DESC = ("batch128: 128 channels 50-350 MHz, each into its own 2048^2 "
+              "complex64 grid with its own cube (64 w-planes, support 3->24 "
+              "scaled by frequency, oversample 4); 256 stations in a 10 km "
+              "disk x 60 samples (1,958,400 visibilities per channel before "
+              "seeded 0-70% flagging)")
+
+
+def run_batch128(args, world, rank, local):
+    """Batched gridding of 128 uneven channels in one graph-captured
+    pipeline (FP16 kernels, compensated FP32 accumulation) against the same
+    channels as 128 sequential plain FP32 jobs."""
+    import ctypes as C
+    import fpga_gridding_b200 as fg
+    from fpga_gridding_b200 import _lib, workloads as W
+
+    lib = fg.load()
+    chans = [c.to(dtype=torch.float32) for c in
+             W.batch_channels(seed=2 + rank, device="cuda")]
+    n_total = sum(c.num_points for c in chans)
+    ws = fg.Workspace(local)
+    s = torch.cuda.Stream()
+    torch.cuda.synchronize()
+
+    def make_jobs(kernel_type):
+        cubes = [fg.Cube(ws, c.support, c.oversample, c.conv_size_half,
+                         c.conv_func, data_is_double=False,
+                         kernel_type=kernel_type) for c in chans]
+        jobs = [dict(cube=cb, uu=c.uu, vv=c.vv, ww=c.ww, vis=c.vis,
+                     weight=c.weight,
+                     cell_size_rad=float(np.float32(c.cell_size_rad)),
+                     w_scale=float(np.float32(c.w_scale)),
+                     grid_size=c.grid_size,
+                     grid=torch.zeros(2 * c.grid_size ** 2,
+                                      dtype=torch.float32, device="cuda"),
+                     d_num_skipped=torch.zeros(1, dtype=torch.int64,
+                                               device="cuda"),
+                     d_norm=torch.zeros(1, dtype=torch.float64, device="cuda"))
+                for c, cb in zip(chans, cubes)]
+        return cubes, jobs
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        s.synchronize()
+        barrier(world)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(args.steps):
+            fn()
+        e1.record(s)
+        e1.synchronize()
+        return max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
+
+    # (a) 128 sequential plain FP32 jobs
+    cubes32, jobs32 = make_jobs(_lib.KERNEL_NATIVE)
+    plain = fg.options()
+
+    def sequential():
+        for j in jobs32:
+            fg.grid_device(ws, j["cube"], j["uu"], j["vv"], j["ww"], j["vis"],
+                           j["weight"], j["cell_size_rad"], j["w_scale"],
+                           j["grid_size"], j["grid"], j["d_num_skipped"],
+                           j["d_norm"], opts=plain, stream=s)
+    seq_ms = timed(sequential)
+
+    # (b) one batch, FP32 plain (same arithmetic as (a)), graph-captured
+    def graph_of(jobs, opts):
+        fg.grid_batch_device(ws, jobs, opts=opts, stream=s)  # sizes buffers
+        s.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=s):
+            fg.grid_batch_device(ws, jobs, opts=opts, stream=s)
+        return g
+    g32 = graph_of(jobs32, plain)
+    batch32_ms = timed(g32.replay)
+    del g32
+    for cb in cubes32:
+        cb.close()
+
+    # (c) one batch, FP16 kernels + compensated accumulation, graph-captured
+    cubes16, jobs16 = make_jobs(_lib.KERNEL_F16)
+    comp = fg.options(accum_mode=_lib.ACCUM_COMPENSATED)
+    g16 = graph_of(jobs16, comp)
+    clocks = ClockSampler(local)
+    clocks.start()
+    batch16_ms = timed(g16.replay)
+    clk = clocks.stop()
+    del g16
+    lib.oskar_b200_set_stage_timing(ws.handle, 1)
+    fg.grid_batch_device(ws, jobs16, opts=comp, stream=s)
+    s.synchronize()
+    st = ws.stats()
+    lib.oskar_b200_set_stage_timing(ws.handle, 0)
+
+    err = {}
+    if rank == 0 and not args.no_cpu_baseline:
+        err = audit_batch(chans, cubes16, ws)
+    for cb in cubes16:
+        cb.close()
+    value = n_total * world / (batch16_ms * 1e-3) / 1e9
+    return {"metric": METRIC, "value": round(value, 4), "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(batch16_ms, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f16 kernels, f32",
+            "data": DATA_DESC,
+            "config": {"workload": BATCH_DESC, "num_points": n_total,
+                       "channels": len(chans),
+                       "mode": "one graph-captured batch: FP16 kernels, "
+                               "compensated FP32 accumulation"},
+            "sequential_plain_fp32_ms": round(seq_ms, 3),
+            "batched_plain_fp32_ms": round(batch32_ms, 3),
+            "speedup_vs_sequential_plain_fp32": round(seq_ms / batch16_ms, 3),
+            "grid_updates_per_s": st.grid_updates * world / (batch16_ms * 1e-3),
+            "stage_ms": {"prep": round(st.prep_ms, 3),
+                         "sort": round(st.sort_ms, 3),
+                         "permute_tasks": round(st.tasks_ms, 3),
+                         "grid_and_fold": round(st.grid_ms, 3)},
+            "gpu_launches_per_step": st.kernel_launches,
+            "rel_err_vs_fp64": err, "clocks": clk}
+
+
+def audit_batch(chans, cubes, ws, m=100000):
+    """Relative RMS vs the FP64 oracle of the batched FP16/compensated path on
+    seeded samples of the lowest and highest channel."""
+    import fpga_gridding_b200 as fg
+    from fpga_gridding_b200 import _lib
+    O = ensure_oracle()
+    out = {}
+    for idx in (0, len(chans) - 1):
+        c = chans[idx]
+        rng = np.random.default_rng(11 + idx)
+        sel = torch.as_tensor(np.sort(rng.choice(c.num_points,
+                                                 size=min(m, c.num_points),
+                                                 replace=False)),
+                              device=c.uu.device)
+        sub = c.subset(sel)
+        hd = host_dict(sub)
+        sd = dict(hd)
+        for k in ("conv_func", "uu", "vv", "ww", "vis", "weight"):
+            sd[k] = np.asarray(hd[k], np.float64)
+        _, n_ref, g_ref = O.grid_d(sd, threads=host_threads())
+        grid = torch.zeros(2 * c.grid_size ** 2, device="cuda")
+        norm = torch.zeros(1, dtype=torch.float64, device="cuda")
+        fg.grid_batch_device(ws, [dict(
+            cube=cubes[idx], uu=sub.uu, vv=sub.vv, ww=sub.ww, vis=sub.vis,
+            weight=sub.weight, cell_size_rad=hd["cell_size_rad"],
+            w_scale=hd["w_scale"], grid_size=c.grid_size, grid=grid,
+            d_norm=norm)], opts=fg.options(accum_mode=_lib.ACCUM_COMPENSATED))
+        torch.cuda.synchronize()
+        out[f"channel_{idx}"] = {
+            "grid_rel_rms": O.rel_rms(grid.cpu().numpy(), g_ref),
+            "norm_rel": abs(norm.item() - n_ref) / abs(n_ref),
+            "sample": f"{len(sel)} seeded visibilities"}
+    return out
+
+
+SERVING_DESC = ("serving: 2000 jobs, visibilities log-uniform in 1e4-5e7, "
+                "grids {512,1024,2048,4096,8192}^2 FP32, 8-256 w-planes, "
+                "support 3-32, FP16 kernel cubes (20% shared), seeded Poisson "
+                "arrivals at 70% of measured capacity, 150 GB HBM budget")
+
+
+def run_serving(args, world, rank, local):
+    """Resident server under a Poisson stream: jobs/s, p50/p99 latency,
+    isolated-job latency, and an audit of 5% of the jobs (mix vs alone, and
+    the FP64 oracle where the job is small enough)."""
+    import fpga_gridding_b200 as fg
+    from fpga_gridding_b200 import _lib, workloads as W
+    from fpga_gridding_b200.serving import Server
+
+    num_jobs = args.serving_jobs
+    base, jobs, specs = W.serving_stream(num_jobs=num_jobs, seed=4 + rank,
+                                         device="cuda")
+    ws = fg.Workspace(local)
+    cubes = {}
+    for key, (sup, csh) in specs.items():
+        cube = W.analytic_kernel_cube(sup, 4, csh, device="cuda").float()
+        cubes[key] = fg.Cube(ws, sup, 4, csh, cube, data_is_double=False,
+                             kernel_type=_lib.KERNEL_F16)
+        del cube
+    torch.cuda.synchronize()
+    srv = Server(local, budget_bytes=150 << 30, slots=4, max_batch=32)
+
+    def submit(i):
+        j = jobs[i]
+        s, e = j["start"], j["start"] + j["n"]
+        srv.submit(i, cubes[j["cube_key"]], base["uu"][s:e], base["vv"][s:e],
+                   base["ww"][s:e], base["vis"][2 * s:2 * e],
+                   base["weight"][s:e], j["cell_size_rad"], j["w_scale"],
+                   j["grid_size"])
+
+    rng = np.random.default_rng(123 + rank)
+    audited = set(rng.choice(num_jobs, size=max(1, num_jobs // 20),
+                             replace=False).tolist())
+    alone_grids = {}
+
+    def drain(pending, keep=None):
+        out = {}
+        while pending:
+            for c in srv.poll(timeout=1.0):
+                if c["status"] != 0:
+                    raise RuntimeError(f"job {c['tag']} status {c['status']}")
+                if keep is not None and c["tag"] in keep:
+                    keep[c["tag"]] = srv.grid(c).cpu().numpy()
+                srv.release(c["tag"])
+                out[c["tag"]] = c
+                pending.discard(c["tag"])
+        return out
+
+    # warm-up, then capacity: every job submitted at once
+    warm = set(range(min(16, num_jobs)))
+    for i in warm:
+        submit(i)
+    drain(set(warm))
+    cap_set = set(range(num_jobs))
+    t0 = srv.clock()
+    for i in cap_set:
+        submit(i)
+    done = drain(set(cap_set))
+    cap_time = max(c["end_s"] for c in done.values()) - t0
+    capacity = num_jobs / cap_time
+    # isolated latency: one job at a time
+    iso = {}
+    for i in range(num_jobs):
+        submit(i)
+        keep = {i: None} if i in audited else None
+        c = drain({i}, keep)[i]
+        iso[i] = c["end_s"] - c["submit_s"]
+        if keep:
+            alone_grids[i] = keep[i]
+    # Poisson arrivals at 70% of capacity
+    rate = 0.7 * capacity
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=num_jobs))
+    mix_grids = {i: None for i in audited}
+    lat, batch_sizes, mem_peak = {}, [], 0
+    start = srv.clock()
+    nxt = 0
+    pending = set()
+    while nxt < num_jobs or pending:
+        now = srv.clock() - start
+        while nxt < num_jobs and arrivals[nxt] <= now:
+            submit(nxt)
+            pending.add(nxt)
+            nxt += 1
+        wait = max(0.0, arrivals[nxt] - (srv.clock() - start)) if nxt < num_jobs else 0.5
+        for c in srv.poll(timeout=min(wait, 0.5)):
+            if c["status"] != 0:
+                raise RuntimeError(f"job {c['tag']} status {c['status']}")
+            if c["tag"] in mix_grids:
+                mix_grids[c["tag"]] = srv.grid(c).cpu().numpy()
+            lat[c["tag"]] = c["end_s"] - c["submit_s"]
+            batch_sizes.append(c["batch_size"])
+            srv.release(c["tag"])
+            pending.discard(c["tag"])
+        mem_peak = max(mem_peak, srv.memory()[0])
+    span = srv.clock() - start
+    srv.close()
+    lat_v = np.array([lat[i] for i in range(num_jobs)])
+    iso_v = np.array([iso[i] for i in range(num_jobs)])
+    ratio = lat_v / iso_v
+    points = sum(j["n"] for j in jobs)
+
+    # audit: mix vs alone for 5% of the jobs, FP64 oracle for the small ones
+    from oracle.oracle import rel_rms
+    same = [rel_rms(mix_grids[i], alone_grids[i]) for i in sorted(audited)]
+    oracle_err = []
+    if not args.no_cpu_baseline:
+        O = ensure_oracle()
+        for i in sorted(audited):
+            j = jobs[i]
+            if j["n"] > 300000:
+                continue
+            s, e = j["start"], j["start"] + j["n"]
+            sup, csh = specs[j["cube_key"]]
+            d = dict(num_w_planes=len(sup), support=sup, oversample=4,
+                     conv_size_half=csh,
+                     conv_func=W.analytic_kernel_cube(sup, 4, csh).float()
+                     .double().numpy(),
+                     uu=base["uu"][s:e].double().cpu().numpy(),
+                     vv=base["vv"][s:e].double().cpu().numpy(),
+                     ww=base["ww"][s:e].double().cpu().numpy(),
+                     vis=base["vis"][2 * s:2 * e].double().cpu().numpy(),
+                     weight=np.ones(j["n"]), cell_size_rad=j["cell_size_rad"],
+                     w_scale=j["w_scale"], grid_size=j["grid_size"])
+            _, _, ref = O.grid_d(d, threads=host_threads())
+            oracle_err.append(rel_rms(alone_grids[i], ref))
+    for c in cubes.values():
+        c.close()
+    ws.close()
+    pct = lambda a, q: float(np.percentile(a, q))
+    return {"metric": METRIC, "value": round(points / span / 1e9, 4),
+            "unit": UNIT, "n_gpus": world, "steps": num_jobs, "warmup": 16,
+            "ms_per_step": round(1e3 * span / num_jobs, 3),
+            "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f16 kernels, f32", "data": DATA_DESC,
+            "config": {"workload": SERVING_DESC, "jobs": num_jobs,
+                       "points": points, "slots": 4, "max_batch": 32},
+            "capacity_jobs_per_s": capacity,
+            "offered_jobs_per_s": rate,
+            "achieved_jobs_per_s": num_jobs / span,
+            "latency_s": {"p50": pct(lat_v, 50), "p99": pct(lat_v, 99)},
+            "isolated_latency_s": {"p50": pct(iso_v, 50), "p99": pct(iso_v, 99)},
+            "slowdown_vs_isolated": {"p50": pct(ratio, 50),
+                                     "p99": pct(ratio, 99)},
+            "p99_latency_over_p99_isolated": pct(lat_v, 99) / pct(iso_v, 99),
+            "mean_batch_size": float(np.mean(batch_sizes)),
+            "server_memory_peak_bytes": mem_peak,
+            "audit": {"jobs": len(audited),
+                      "mix_vs_alone_rel_rms_max": max(same) if same else None,
+                      "fp64_oracle_rel_rms_max": max(oracle_err) if oracle_err else None,
+                      "fp64_oracle_jobs": len(oracle_err)}}
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return None
@@ -489,6 +803,13 @@ def main():
                     help="target wall time of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", choices=("plain_large", "batch128",
+                                           "serving"),
+                    default="plain_large",
+                    help="plain_large (the benchmark job), batch128 (the "
+                         "128-channel batching workload) or serving (the "
+                         "Poisson job stream)")
+    ap.add_argument("--serving-jobs", type=int, default=2000)
     ap.add_argument("--stations", type=int, default=512,
                     help="stations of the job (512 = the benchmark job; "
                          "fewer = a smaller profiling case)")
@@ -504,7 +825,12 @@ def main():
         return
     world, rank, local = dist_setup(args.gpus)
     try:
-        out = run_b200(args, world, rank, local)
+        if args.workload == "batch128":
+            out = run_batch128(args, world, rank, local)
+        elif args.workload == "serving":
+            out = run_serving(args, world, rank, local)
+        else:
+            out = run_b200(args, world, rank, local)
         if rank == 0 and out is not None:
             print(json.dumps(out), flush=True)
     finally:

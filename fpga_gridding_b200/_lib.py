@@ -24,10 +24,18 @@ EXPORTED_SYMBOLS = (
     "oskar_b200_cube_free",
     "oskar_b200_cube_bytes",
     "oskar_b200_grid",
+    "oskar_b200_grid_batch",
     "oskar_b200_place",
     "oskar_b200_last_stats",
     "oskar_b200_set_stage_timing",
     "oskar_b200_measure_atomic_rate",
+    "oskar_b200_server_create",
+    "oskar_b200_server_submit",
+    "oskar_b200_server_poll",
+    "oskar_b200_server_release",
+    "oskar_b200_server_clock",
+    "oskar_b200_server_memory",
+    "oskar_b200_server_free",
     "oskar_b200_build_info",
 )
 
@@ -55,7 +63,7 @@ class Options(C.Structure):
     _fields_ = [("coord_mode", C.c_int), ("kernel_type", C.c_int),
                 ("accum_mode", C.c_int), ("apply_weight", C.c_int),
                 ("classes_per_thread", C.c_int), ("staging", C.c_int),
-                ("reserved", C.c_int * 10)]
+                ("compensate_radius", C.c_int), ("reserved", C.c_int * 9)]
 
 
 class Stats(C.Structure):
@@ -70,6 +78,32 @@ class Stats(C.Structure):
 _P = C.c_void_p
 _SZ = C.c_size_t
 _lib = None
+
+
+class Request(C.Structure):
+    """oskar_B200Request: one job submitted to a server."""
+    _fields_ = [("tag", C.c_ulonglong), ("cube", _P), ("num_points", _SZ),
+                ("uu", _P), ("vv", _P), ("ww", _P), ("vis", _P),
+                ("weight", _P), ("cell_size_rad", C.c_double),
+                ("w_scale", C.c_double), ("grid_size", C.c_int)]
+
+
+class Completion(C.Structure):
+    """oskar_B200Completion."""
+    _fields_ = [("tag", C.c_ulonglong), ("status", C.c_int),
+                ("num_skipped", C.c_ulonglong), ("norm", C.c_double),
+                ("grid", _P), ("submit_s", C.c_double),
+                ("start_s", C.c_double), ("end_s", C.c_double),
+                ("batch_size", C.c_int)]
+
+
+class Job(C.Structure):
+    """oskar_B200Job: one job of oskar_b200_grid_batch."""
+    _fields_ = [("cube", _P), ("num_points", _SZ), ("uu", _P), ("vv", _P),
+                ("ww", _P), ("vis", _P), ("weight", _P),
+                ("cell_size_rad", C.c_double), ("w_scale", C.c_double),
+                ("grid_size", C.c_int), ("grid", _P), ("d_num_skipped", _P),
+                ("d_norm", _P)]
 
 
 def load():
@@ -115,9 +149,27 @@ def load():
     lib.oskar_b200_set_stage_timing.argtypes = [_P, C.c_int]
     lib.oskar_b200_measure_atomic_rate.argtypes = [
         _P, _P, C.c_int, C.c_int, C.POINTER(C.c_double)]
+    lib.oskar_b200_grid_batch.argtypes = [_P, C.POINTER(Options), C.c_int,
+                                          C.POINTER(Job), _P]
+    lib.oskar_b200_server_create.argtypes = [C.c_int, _SZ, C.c_int, C.c_int,
+                                             C.POINTER(Options),
+                                             C.POINTER(_P)]
+    lib.oskar_b200_server_submit.argtypes = [_P, C.POINTER(Request)]
+    lib.oskar_b200_server_poll.argtypes = [_P, C.POINTER(Completion), C.c_int,
+                                           C.POINTER(C.c_int), C.c_double]
+    lib.oskar_b200_server_release.argtypes = [_P, C.c_ulonglong]
+    lib.oskar_b200_server_clock.argtypes = [_P]
+    lib.oskar_b200_server_clock.restype = C.c_double
+    lib.oskar_b200_server_memory.argtypes = [_P, C.POINTER(_SZ),
+                                             C.POINTER(_SZ)]
+    lib.oskar_b200_server_free.argtypes = [_P]
+    for name in ("oskar_b200_server_create", "oskar_b200_server_submit",
+                 "oskar_b200_server_poll", "oskar_b200_server_release",
+                 "oskar_b200_server_memory", "oskar_b200_server_free"):
+        getattr(lib, name).restype = C.c_int
     for name in ("oskar_b200_workspace_create", "oskar_b200_workspace_free",
                  "oskar_b200_cube_create", "oskar_b200_cube_free",
-                 "oskar_b200_grid",
+                 "oskar_b200_grid", "oskar_b200_grid_batch",
                  "oskar_b200_place", "oskar_b200_last_stats",
                  "oskar_b200_set_stage_timing",
                  "oskar_b200_measure_atomic_rate"):

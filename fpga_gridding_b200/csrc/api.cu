@@ -97,6 +97,8 @@ void workspace_free(oskar_B200Workspace* ws)
     if (ws->stream) cudaStreamSynchronize(ws->stream);
     for (cudaEvent_t& e : ws->events)
         if (e) cudaEventDestroy(e);
+    if (ws->jobs_event) cudaEventDestroy(ws->jobs_event);
+    if (ws->h_jobs) cudaFreeHost(ws->h_jobs);
     if (ws->h_counters) cudaFreeHost(ws->h_counters);
     if (ws->stream) cudaStreamDestroy(ws->stream);
     delete ws;  // DeviceBuffer destructors free device memory
@@ -512,6 +514,40 @@ int oskar_b200_grid(oskar_B200Workspace* ws, const oskar_B200Cube* cube,
     return run_grid(ws, cube, opt, num_points, uu, vv, ww, vis, weight,
                     cell_size_rad, w_scale, grid_size, grid, d_num_skipped,
                     d_norm, s);
+}
+
+int oskar_b200_grid_batch(oskar_B200Workspace* ws,
+                          const oskar_B200Options* opt, int num_jobs,
+                          const oskar_B200Job* jobs, void* stream)
+{
+    if (!ws || !jobs || num_jobs < 1 || num_jobs > (1 << 15))
+        return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    oskar_B200Options defaults;
+    oskar_b200_options_init(&defaults);
+    if (!opt) opt = &defaults;
+    const oskar_B200Cube* c0 = jobs[0].cube;
+    if (!c0) return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    int st = check_options(opt, c0->data_is_double);
+    if (st) return st;
+    std::vector<HostJob> hj((size_t)num_jobs);
+    for (int j = 0; j < num_jobs; ++j)
+    {
+        const oskar_B200Job& in = jobs[j];
+        if (!in.cube || in.cube->device != ws->device ||
+            in.cube->data_is_double != c0->data_is_double ||
+            in.cube->kernel_type != c0->kernel_type)
+            return OSKAR_B200_ERR_INVALID_ARGUMENT;
+        st = check_grid_args(in.num_points, in.uu, in.vv, in.ww, in.vis,
+                             in.weight, opt->apply_weight, in.grid_size,
+                             in.grid);
+        if (st) return st;
+        hj[j] = HostJob{in.cube, in.num_points, in.uu, in.vv, in.ww, in.vis,
+                        in.weight, in.cell_size_rad, in.w_scale,
+                        in.grid_size, in.grid, in.d_num_skipped, in.d_norm};
+    }
+    DeviceGuard g(ws->device);
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ws->stream;
+    return run_batch(ws, opt, num_jobs, hj.data(), s);
 }
 
 int oskar_b200_place(oskar_B200Workspace* ws, int data_is_double,

@@ -228,9 +228,15 @@ struct CompensatedFlush
 {
     float* grid;
     float* comp;
+    bool active;   // false: this task's cells are not compensated
     __device__ __forceinline__ void operator()(bool pred, unsigned cell,
                                                float re, float im) const
     {
+        if (!active)
+        {
+            red_add_c_if(pred, grid + 2 * (size_t)cell, re, im);
+            return;
+        }
         if (!pred) return;
         float ore, oim;
         asm volatile("atom.relaxed.gpu.global.add.v2.f32 {%0, %1}, [%2], {%3, %4};"
@@ -341,21 +347,23 @@ template <> struct FlushFor<float, true> { using type = CompensatedFlush; };
 
 template <typename GT, bool COMP>
 __device__ __forceinline__ typename FlushFor<GT, COMP>::type
-make_flush(void* grid, void* comp);
+make_flush(void* grid, void* comp, bool active);
 template <>
-__device__ __forceinline__ PlainFlush<float> make_flush<float, false>(void* grid, void*)
+__device__ __forceinline__ PlainFlush<float> make_flush<float, false>(void* grid, void*, bool)
 {
     return PlainFlush<float>{static_cast<float*>(grid)};
 }
 template <>
-__device__ __forceinline__ PlainFlush<double> make_flush<double, false>(void* grid, void*)
+__device__ __forceinline__ PlainFlush<double> make_flush<double, false>(void* grid, void*, bool)
 {
     return PlainFlush<double>{static_cast<double*>(grid)};
 }
 template <>
-__device__ __forceinline__ CompensatedFlush make_flush<float, true>(void* grid, void* comp)
+__device__ __forceinline__ CompensatedFlush make_flush<float, true>(void* grid, void* comp,
+                                                                    bool active)
 {
-    return CompensatedFlush{static_cast<float*>(grid), static_cast<float*>(comp)};
+    return CompensatedFlush{static_cast<float*>(grid), static_cast<float*>(comp),
+                            active};
 }
 
 template <typename GT, typename KT, bool STAGED, bool COMP>
@@ -374,12 +382,8 @@ romein_grid_kernel(const GridArgs a)
     __shared__ int s_run_begin[kMaxOffsets], s_run_end[kMaxOffsets];
 
     const V2* __restrict__ svis = static_cast<const V2*>(a.svis);
-    const KT* __restrict__ slabs = static_cast<const KT*>(a.slabs);
-    const auto fl = make_flush<GT, COMP>(a.grid, a.comp);
     unsigned long long* status = &a.counters[CNT_STATUS];
     const unsigned num_tasks = (unsigned)a.counters[CNT_TASKS];
-    const unsigned cells = (unsigned)a.grid_size * (unsigned)a.grid_size;
-    const int offsets = 2 * a.half + 1;
 
     if (STAGED && threadIdx.x == 0)
     {
@@ -394,7 +398,7 @@ romein_grid_kernel(const GridArgs a)
     {
         if (threadIdx.x == 0)
             s_task = (unsigned)atomicAdd(&a.counters[CNT_TASK_NEXT], 1ull);
-        if (threadIdx.x < offsets)
+        if (threadIdx.x < kMaxOffsets)
         {
             s_run_begin[threadIdx.x] = 0;
             s_run_end[threadIdx.x] = 0;
@@ -412,8 +416,25 @@ romein_grid_kernel(const GridArgs a)
                 atomicOr(status, (unsigned long long)DEV_ERR_TASK);
             continue;
         }
+        // The task's job: its cube, grid and geometry.
+        const JobDesc& jd = a.jobs[a.task_job[task]];
+        const KT* __restrict__ slabs = static_cast<const KT*>(jd.slabs);
+        // Compensation is limited to tasks near the grid centre when a
+        // radius is set (a task is a compact run of one coarse tile).
+        bool comp_here = true;
+        if (COMP && a.comp_radius > 0)
+        {
+            const int4 r0 = a.srec[begin];
+            const int c = jd.grid_size / 2;
+            comp_here = abs(r0.x - c) <= a.comp_radius &&
+                        abs(r0.y - c) <= a.comp_radius;
+        }
+        const auto fl = make_flush<GT, COMP>(jd.grid, jd.comp, comp_here);
+        const int grid_size = jd.grid_size;
+        const unsigned cells = (unsigned)grid_size * (unsigned)grid_size;
+        const int offsets = 2 * jd.half + 1;
         const int plane = a.srec[begin].z & 0x7fffffff;
-        const PlaneDesc d = a.planes[plane];
+        const PlaneDesc d = static_cast<const PlaneDesc*>(jd.planes)[plane];
         const int w = 2 * d.support + 1;
         const int cpt = d.support < kTuneMax ? a.cpt[d.support] : 5;
 
@@ -426,7 +447,7 @@ romein_grid_kernel(const GridArgs a)
         {
             const int src = (int)(key & 0xffu);
             s_vis[t] = derive<GT>(a.srec[begin + src], svis[begin + src], d,
-                                  a.grid_size, a.oversample, a.half, status);
+                                  grid_size, jd.oversample, jd.half, status);
             s_order[t] = key;
         }
         __syncthreads();
@@ -443,7 +464,7 @@ romein_grid_kernel(const GridArgs a)
         if (!STAGED)
         {
             dispatch_cpt<GT, KT>(cpt, s_vis, m, w, d.pitch, 0,
-                                 slabs + d.offset, fl, a.grid_size, cells,
+                                 slabs + d.offset, fl, grid_size, cells,
                                  flushes);
             continue;
         }
@@ -478,7 +499,7 @@ romein_grid_kernel(const GridArgs a)
             phase ^= 1u;
             dispatch_cpt<GT, KT>(cpt, s_vis + rb, re - rb, w, d.pitch,
                                  ov * (int)block_elems, s_block, fl,
-                                 a.grid_size, cells, flushes);
+                                 grid_size, cells, flushes);
             __syncthreads();
         }
     }
@@ -575,9 +596,14 @@ void default_tune_table(unsigned char* cpt)
 
 namespace {
 
-__global__ void fold_kernel(float2* __restrict__ grid, float2* __restrict__ comp,
-                            size_t cells)
+// Block (x, j) folds part of job j's error grid into its grid.
+__global__ void fold_kernel(const JobDesc* __restrict__ jobs)
 {
+    const JobDesc& jd = jobs[blockIdx.y];
+    if (!jd.comp) return;
+    float2* grid = static_cast<float2*>(jd.grid);
+    float2* comp = static_cast<float2*>(jd.comp);
+    const size_t cells = (size_t)jd.grid_size * (size_t)jd.grid_size;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < cells;
          i += (size_t)gridDim.x * blockDim.x)
     {
@@ -595,38 +621,40 @@ __global__ void fold_kernel(float2* __restrict__ grid, float2* __restrict__ comp
 
 }  // namespace
 
-cudaError_t launch_fold(float* grid, float* comp, size_t cells, int num_sms,
-                        cudaStream_t st)
+cudaError_t launch_fold_jobs(const JobDesc* jobs, int num_jobs, int num_sms,
+                             cudaStream_t st)
 {
-    fold_kernel<<<num_sms * 8, 256, 0, st>>>(reinterpret_cast<float2*>(grid),
-                                            reinterpret_cast<float2*>(comp),
-                                            cells);
+    int bx = num_sms * 8 / (num_jobs > 0 ? num_jobs : 1);
+    if (bx < 4) bx = 4;
+    fold_kernel<<<dim3(bx, num_jobs), 256, 0, st>>>(jobs);
     return cudaGetLastError();
 }
 
-size_t grid_smem_bytes(const oskar_B200Cube* cube, bool staged)
+size_t grid_smem_bytes(int data_is_double, unsigned max_block_bytes,
+                       bool staged)
 {
-    const size_t rec = cube->data_is_double ? sizeof(TapVis<double>)
-                                            : sizeof(TapVis<float>);
-    const size_t block = staged ? ((cube->max_block_bytes + 127) / 128) * 128 : 0;
+    const size_t rec = data_is_double ? sizeof(TapVis<double>)
+                                      : sizeof(TapVis<float>);
+    const size_t block = staged ? ((max_block_bytes + 127) / 128) * 128 : 0;
     return block + rec * kTaskMax;
 }
 
-cudaError_t launch_grid(const GridArgs& a, const oskar_B200Cube* cube,
-                        bool staged, bool compensated, int num_sms,
-                        cudaStream_t st, int* ctas_out)
+cudaError_t launch_grid(const GridArgs& a, int data_is_double,
+                        int kernel_type, unsigned max_block_bytes, bool staged,
+                        bool compensated, int num_sms, cudaStream_t st,
+                        int* ctas_out)
 {
-    const size_t smem = grid_smem_bytes(cube, staged);
+    const size_t smem = grid_smem_bytes(data_is_double, max_block_bytes,
+                                        staged);
     GridArgs args = a;
-    args.block_smem_bytes = staged ? (unsigned)(((cube->max_block_bytes + 127) /
+    args.block_smem_bytes = staged ? (unsigned)(((max_block_bytes + 127) /
                                                   128) * 128)
                                     : 0u;
     if (compensated)
     {
         // FP32 grids only; kernel values read through L1.
-        if (cube->data_is_double || staged || !a.comp)
-            return cudaErrorInvalidValue;
-        switch (cube->kernel_type)
+        if (data_is_double || staged) return cudaErrorInvalidValue;
+        switch (kernel_type)
         {
         case OSKAR_B200_KERNEL_F16:
             return launch_variant<float, __half2, false, true>(args, num_sms, smem, st, ctas_out);
@@ -636,14 +664,14 @@ cudaError_t launch_grid(const GridArgs& a, const oskar_B200Cube* cube,
             return launch_variant<float, float2, false, true>(args, num_sms, smem, st, ctas_out);
         }
     }
-    if (cube->data_is_double)
+    if (data_is_double)
     {
-        if (cube->kernel_type != OSKAR_B200_KERNEL_NATIVE)
+        if (kernel_type != OSKAR_B200_KERNEL_NATIVE)
             return cudaErrorInvalidValue;
         return staged ? launch_variant<double, double2, true>(args, num_sms, smem, st, ctas_out)
                       : launch_variant<double, double2, false>(args, num_sms, smem, st, ctas_out);
     }
-    switch (cube->kernel_type)
+    switch (kernel_type)
     {
     case OSKAR_B200_KERNEL_F16:
         return staged ? launch_variant<float, __half2, true>(args, num_sms, smem, st, ctas_out)

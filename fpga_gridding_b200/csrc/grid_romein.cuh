@@ -16,25 +16,23 @@ struct GridArgs
     const int4* srec;           // sorted placement records
     const void* svis;           // sorted visibilities (float2 / double2)
     const uint32_t* task_start; // [num_tasks + 1]
-    const PlaneDesc* planes;
-    const void* slabs;
-    void* grid;
-    void* comp;                 // compensation grid (ACCUM_COMPENSATED) or null
+    const uint32_t* task_job;   // [num_tasks]: job of each task
+    const JobDesc* jobs;        // cube, grid and geometry of each job
     unsigned long long* counters;
-    int grid_size;
-    int oversample;
-    int half;
     unsigned block_smem_bytes;  // set by launch_grid
+    int comp_radius;            // see oskar_B200Options::compensate_radius
     unsigned char cpt[kTuneMax];
 };
 
 void default_tune_table(unsigned char* cpt);
-size_t grid_smem_bytes(const oskar_B200Cube* cube, bool staged);
-cudaError_t launch_grid(const GridArgs& a, const oskar_B200Cube* cube,
-                        bool staged, bool compensated, int num_sms,
-                        cudaStream_t st, int* ctas_out);
-// grid[i] += comp[i]; comp[i] = 0 over 2 * cells floats.
-cudaError_t launch_fold(float* grid, float* comp, size_t cells,
-                        int num_sms, cudaStream_t st);
+size_t grid_smem_bytes(int data_is_double, unsigned max_block_bytes,
+                       bool staged);
+cudaError_t launch_grid(const GridArgs& a, int data_is_double,
+                        int kernel_type, unsigned max_block_bytes, bool staged,
+                        bool compensated, int num_sms, cudaStream_t st,
+                        int* ctas_out);
+// For every job with an error grid: grid += comp, comp = 0.
+cudaError_t launch_fold_jobs(const JobDesc* jobs, int num_jobs, int num_sms,
+                             cudaStream_t st);
 
 }  // namespace b200

@@ -39,6 +39,35 @@ struct PlaneDesc
     float scale;        // stored value = true value / scale (1 unless F16/BF16)
 };
 
+// One gridding job of a batch, as the device kernels see it.  A single
+// oskar_b200_grid call is a batch of one.
+struct JobDesc
+{
+    const void* uu;
+    const void* vv;
+    const void* ww;
+    const void* vis;
+    const void* weight;
+    void* grid;
+    void* comp;                   // error grid (ACCUM_COMPENSATED) or null
+    const PlaneDesc* planes;
+    const void* slabs;
+    const double* norm_table;
+    const int* support;
+    double* d_norm;               // caller's norm accumulator (device) or null
+    unsigned long long* d_skipped;// caller's skip count (device) or null
+    double grid_scale;            // grid_size * cell_size_rad, FP64
+    double w_scale;
+    float grid_scale_f;           // the same rounded as float C computes it
+    float w_scale_f;
+    unsigned long long first;     // global index of the job's first point
+    unsigned long long n;         // points of the job
+    int grid_size;
+    int num_planes;
+    int oversample;
+    int half;                     // ceil(oversample / 2)
+};
+
 struct DeviceBuffer
 {
     void* ptr = nullptr;
@@ -49,6 +78,11 @@ struct DeviceBuffer
     DeviceBuffer() = default;
     DeviceBuffer(const DeviceBuffer&) = delete;
     DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    DeviceBuffer(DeviceBuffer&& o) noexcept : ptr(o.ptr), bytes(o.bytes)
+    {
+        o.ptr = nullptr;
+        o.bytes = 0;
+    }
 };
 
 // Grid-launch tuning for one support size (the "autotuner" table entry).
@@ -68,9 +102,16 @@ struct oskar_B200Workspace
     cudaStream_t stream = nullptr;
     // per-visibility work arrays
     b200::DeviceBuffer keys[2], vals[2], rec, srec, svis, scan_tmp, flags;
-    b200::DeviceBuffer task_start;
-    // small arrays: counters, partial sums, plane histogram
-    b200::DeviceBuffer counters, partials, plane_counts;
+    b200::DeviceBuffer task_start, task_job;
+    // small arrays: counters, partial sums, per-job plane histograms and
+    // skip counts, the job table
+    b200::DeviceBuffer counters, partials, plane_counts, job_skipped, jobs;
+    // pinned host copy of the job table (the source of its upload), and the
+    // event after which the upload has read it
+    void* h_jobs = nullptr;
+    size_t h_jobs_bytes = 0;
+    cudaEvent_t jobs_event = nullptr;
+    int jobs_event_pending = 0;
     // drop-in staging of the caller's host arrays
     b200::DeviceBuffer in_uu, in_vv, in_ww, in_vis, in_weight, in_grid,
         in_cube, in_norm;
@@ -134,6 +175,9 @@ int cube_build(oskar_B200Cube* cube, const void* d_conv_func,
                int conv_func_is_double, cudaStream_t st);
 
 // ---- prep.cu / grid_romein.cu ---------------------------------------------
+// Sort key, most significant first:
+//   job | coarse tile (Morton) | w-plane | cell inside the tile (Morton)
+// with a skip flag above all of them.
 struct KeyLayout
 {
     int coarse_shift;  // log2 of the coarse tile side (cells)
@@ -141,9 +185,37 @@ struct KeyLayout
     int fine_shift;    // cells dropped inside a coarse tile
     int fine_bits;     // bits per axis of the fine index
     int plane_bits;
+    int job_bits;
+    int job_shift;     // position of the job field
     int total_bits;    // key bits below the skip flag
 };
-KeyLayout make_key_layout(int grid_size, int num_planes);
+// Layout for the largest grid and plane count of the batch; false if the
+// fields cannot fit 31 bits.
+bool make_key_layout(int grid_size, int num_planes, int num_jobs,
+                     KeyLayout* out);
+
+// One job of a batch, host side.
+struct HostJob
+{
+    const oskar_B200Cube* cube;
+    size_t num_points;
+    const void* uu;
+    const void* vv;
+    const void* ww;
+    const void* vis;
+    const void* weight;
+    double cell_size_rad;
+    double w_scale;
+    int grid_size;
+    void* grid;
+    unsigned long long* d_num_skipped;
+    double* d_norm;
+};
+
+// Grids a batch of jobs that share precision and kernel storage type, with
+// one sort and one persistent gridding launch.
+int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
+              int num_jobs, const HostJob* jobs, cudaStream_t st);
 
 int run_grid(oskar_B200Workspace* ws, const oskar_B200Cube* cube,
              const oskar_B200Options* opt, size_t num_points, const void* uu,

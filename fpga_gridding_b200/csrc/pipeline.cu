@@ -1,11 +1,13 @@
-// One gridding job on device-resident data:
-//   prep (placement, keys, norm, skip count, plane histogram)
-//   -> radix sort of (key, index)
+// Gridding of a batch of jobs on device-resident data:
+//   prep (placement, keys, norms, skip counts, plane histograms)
+//   -> one radix sort of (key, index) over all jobs (job in the top bits)
 //   -> permute records and visibilities into sorted order
-//   -> task list
-//   -> Romein gridding kernel.
+//   -> task list (tasks never cross a job, tile or plane)
+//   -> one persistent Romein gridding launch over every task of every job.
+// A single oskar_b200_grid call is a batch of one job.
 #include <algorithm>
 #include <cstring>
+#include <vector>
 
 #include "common.cuh"
 #include "grid_romein.cuh"
@@ -55,28 +57,20 @@ void DeviceBuffer::release()
 
 DeviceBuffer::~DeviceBuffer() { release(); }
 
-namespace {
-
-#define B200_TRY(expr)                                   \
-    do {                                                 \
-        const cudaError_t e_ = (expr);                   \
+#define B200_TRY(expr)                                      \
+    do {                                                    \
+        const cudaError_t e_ = (expr);                      \
         if (e_ != cudaSuccess) return status_from_cuda(e_); \
     } while (0)
 
-}  // namespace
-
-int run_grid(oskar_B200Workspace* ws, const oskar_B200Cube* cube,
-             const oskar_B200Options* opt, size_t n, const void* uu,
-             const void* vv, const void* ww, const void* vis,
-             const void* weight, double cell_size_rad, double w_scale,
-             int grid_size, void* grid, unsigned long long* d_num_skipped,
-             double* d_norm, cudaStream_t st)
+int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
+              int num_jobs, const HostJob* jobs, cudaStream_t st)
 {
-    const bool dbl = cube->data_is_double != 0;
-    const int P = cube->num_planes;
+    const oskar_B200Cube* c0 = jobs[0].cube;
+    const bool dbl = c0->data_is_double != 0;
     const size_t vsz = dbl ? sizeof(double) : sizeof(float);
+    const bool comp = opt->accum_mode == OSKAR_B200_ACCUM_COMPENSATED;
     int launches = 0;
-    ws->last_points = n;
     ws->last_launches = 0;
     ws->events_recorded = 0;
     const bool timing = ws->stage_timing != 0;
@@ -84,60 +78,133 @@ int run_grid(oskar_B200Workspace* ws, const oskar_B200Cube* cube,
         return timing ? cudaEventRecord(ws->events[i], st) : cudaSuccess;
     };
 
+    // Job table (host, pinned: it is the source of an async upload).
+    size_t n = 0, max_points = 0, comp_floats = 0;
+    int max_grid = 1, max_planes = 1;
+    unsigned max_block = 0;
+    for (int j = 0; j < num_jobs; ++j)
+    {
+        n += jobs[j].num_points;
+        max_points = std::max(max_points, jobs[j].num_points);
+        max_grid = std::max(max_grid, jobs[j].grid_size);
+        max_planes = std::max(max_planes, jobs[j].cube->num_planes);
+        max_block = std::max(max_block, jobs[j].cube->max_block_bytes);
+        if (comp)
+            comp_floats += 2 * (size_t)jobs[j].grid_size * jobs[j].grid_size;
+    }
+    if (n >= 0xffffffffull) return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    ws->last_points = n;
+    KeyLayout kl;
+    if (!make_key_layout(max_grid, max_planes, num_jobs, &kl))
+        return OSKAR_B200_ERR_UNSUPPORTED;
+    const size_t job_bytes = sizeof(JobDesc) * num_jobs;
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    B200_TRY(cudaStreamIsCapturing(st, &capture));
+    const bool capturing = capture != cudaStreamCaptureStatusNone;
+    // The previous call's upload of the job table must have read it before
+    // it is rewritten.  (A caller capturing a graph has synchronised.)
+    if (ws->jobs_event_pending && !capturing)
+        B200_TRY(cudaEventSynchronize(ws->jobs_event));
+    ws->jobs_event_pending = 0;
+    if (ws->h_jobs_bytes < job_bytes)
+    {
+        if (ws->h_jobs) cudaFreeHost(ws->h_jobs);
+        ws->h_jobs = nullptr;
+        ws->h_jobs_bytes = 0;
+        B200_TRY(cudaMallocHost(&ws->h_jobs, job_bytes));
+        ws->h_jobs_bytes = job_bytes;
+    }
+    if (comp) B200_TRY(ws->comp_grid.ensure(comp_floats * sizeof(float)));
+    JobDesc* hj = static_cast<JobDesc*>(ws->h_jobs);
+    size_t first = 0, comp_off = 0;
+    for (int j = 0; j < num_jobs; ++j)
+    {
+        const HostJob& h = jobs[j];
+        const oskar_B200Cube* c = h.cube;
+        JobDesc d{};
+        d.uu = h.uu;
+        d.vv = h.vv;
+        d.ww = h.ww;
+        d.vis = h.vis;
+        d.weight = h.weight;
+        d.grid = h.grid;
+        d.comp = comp ? static_cast<float*>(ws->comp_grid.ptr) + comp_off
+                      : nullptr;
+        d.planes = static_cast<const PlaneDesc*>(c->d_planes.ptr);
+        d.slabs = c->d_slabs.ptr;
+        d.norm_table = static_cast<const double*>(c->d_norm_table.ptr);
+        d.support = static_cast<const int*>(c->d_support.ptr);
+        d.d_norm = h.d_norm;
+        d.d_skipped = h.d_num_skipped;
+        d.grid_scale = (double)h.grid_size * h.cell_size_rad;
+        d.w_scale = h.w_scale;
+        // The reference's float path computes grid_size * cell_size_rad in
+        // float (oskar_grid_wproj.c:150).
+        d.grid_scale_f = (float)h.grid_size * (float)h.cell_size_rad;
+        d.w_scale_f = (float)h.w_scale;
+        d.first = first;
+        d.n = h.num_points;
+        d.grid_size = h.grid_size;
+        d.num_planes = c->num_planes;
+        d.oversample = c->oversample;
+        d.half = c->half;
+        hj[j] = d;
+        first += h.num_points;
+        if (comp) comp_off += 2 * (size_t)h.grid_size * h.grid_size;
+    }
+    const int bpj = prep_blocks_per_job(max_points, num_jobs, ws->num_sms);
     B200_TRY(ws->counters.ensure(sizeof(unsigned long long) * CNT_COUNT));
-    B200_TRY(ws->plane_counts.ensure(sizeof(unsigned long long) * P));
+    B200_TRY(ws->jobs.ensure(job_bytes));
+    B200_TRY(ws->job_skipped.ensure(sizeof(unsigned long long) * num_jobs));
+    B200_TRY(ws->plane_counts.ensure(sizeof(unsigned long long) * num_jobs *
+                                     max_planes));
+    B200_TRY(ws->partials.ensure(sizeof(double) * num_jobs * bpj));
     unsigned long long* counters =
         static_cast<unsigned long long*>(ws->counters.ptr);
     B200_TRY(cudaMemsetAsync(counters, 0,
                              sizeof(unsigned long long) * CNT_COUNT, st));
+    B200_TRY(cudaMemsetAsync(ws->job_skipped.ptr, 0,
+                             sizeof(unsigned long long) * num_jobs, st));
     B200_TRY(cudaMemsetAsync(ws->plane_counts.ptr, 0,
-                             sizeof(unsigned long long) * P, st));
-    if (n == 0)
+                             sizeof(unsigned long long) * num_jobs * max_planes,
+                             st));
+    B200_TRY(cudaMemcpyAsync(ws->jobs.ptr, hj, job_bytes,
+                             cudaMemcpyHostToDevice, st));
     {
-        if (d_num_skipped)
-            B200_TRY(cudaMemsetAsync(d_num_skipped, 0, sizeof(*d_num_skipped),
-                                     st));
-        B200_TRY(cudaMemcpyAsync(ws->h_counters, counters,
-                                 sizeof(unsigned long long) * CNT_COUNT,
-                                 cudaMemcpyDeviceToHost, st));
-        return OSKAR_B200_OK;
+        // Outside stream capture, remember when the upload has happened.
+        if (!capturing)
+        {
+            if (!ws->jobs_event)
+                B200_TRY(cudaEventCreateWithFlags(&ws->jobs_event,
+                                                  cudaEventDisableTiming));
+            B200_TRY(cudaEventRecord(ws->jobs_event, st));
+            ws->jobs_event_pending = 1;
+        }
+    }
+    const JobDesc* d_jobs = static_cast<const JobDesc*>(ws->jobs.ptr);
+
+    if (n > 0)
+    {
+        B200_TRY(ws->keys[0].ensure(4 * n));
+        B200_TRY(ws->keys[1].ensure(4 * n));
+        B200_TRY(ws->vals[0].ensure(4 * n));
+        B200_TRY(ws->vals[1].ensure(4 * n));
+        B200_TRY(ws->rec.ensure(16 * n));
+        B200_TRY(ws->srec.ensure(16 * n));
+        B200_TRY(ws->svis.ensure(2 * vsz * n));
+        B200_TRY(ws->flags.ensure(4 * n));
+        B200_TRY(ws->task_start.ensure(4 * (n + 2)));
+        B200_TRY(ws->task_job.ensure(4 * (n + 2)));
+        B200_TRY(ws->scan_tmp.ensure(std::max(radix_sort_temp_bytes(n),
+                                              scan_temp_bytes(n))));
     }
 
-    B200_TRY(ws->keys[0].ensure(4 * n));
-    B200_TRY(ws->keys[1].ensure(4 * n));
-    B200_TRY(ws->vals[0].ensure(4 * n));
-    B200_TRY(ws->vals[1].ensure(4 * n));
-    B200_TRY(ws->rec.ensure(16 * n));
-    B200_TRY(ws->srec.ensure(16 * n));
-    B200_TRY(ws->svis.ensure(2 * vsz * n));
-    B200_TRY(ws->flags.ensure(4 * n));
-    B200_TRY(ws->task_start.ensure(4 * (n + 2)));
-    B200_TRY(ws->scan_tmp.ensure(std::max(radix_sort_temp_bytes(n),
-                                          scan_temp_bytes(n))));
-    const unsigned blocks = prep_num_blocks(n, ws->num_sms);
-    B200_TRY(ws->partials.ensure(sizeof(double) * blocks));
-
-    const KeyLayout kl = make_key_layout(grid_size, P);
     PrepArgs pa{};
-    pa.uu = uu;
-    pa.vv = vv;
-    pa.ww = ww;
-    pa.weight = weight;
-    pa.n = n;
-    pa.pc.grid_scale = (double)grid_size * cell_size_rad;
-    pa.pc.w_scale = w_scale;
-    // The reference's float path computes grid_size * cell_size_rad in float.
-    pa.pc.grid_scale_f = (float)grid_size * (float)cell_size_rad;
-    pa.pc.w_scale_f = (float)w_scale;
-    pa.pc.grid_size = grid_size;
-    pa.pc.centre = grid_size / 2;
-    pa.pc.num_planes = P;
-    pa.pc.oversample = cube->oversample;
-    pa.support = static_cast<const int*>(cube->d_support.ptr);
-    pa.num_planes = P;
-    pa.half = cube->half;
+    pa.jobs = d_jobs;
+    pa.num_jobs = num_jobs;
+    pa.blocks_per_job = bpj;
+    pa.max_planes = max_planes;
     pa.apply_weight = opt->apply_weight;
-    pa.norm_table = static_cast<const double*>(cube->d_norm_table.ptr);
     pa.key = kl;
     pa.rec = static_cast<int4*>(ws->rec.ptr);
     uint32_t* keys[2] = {static_cast<uint32_t*>(ws->keys[0].ptr),
@@ -147,72 +214,86 @@ int run_grid(oskar_B200Workspace* ws, const oskar_B200Cube* cube,
     pa.keys = keys[0];
     pa.vals = vals[0];
     pa.counters = counters;
+    pa.job_skipped = static_cast<unsigned long long*>(ws->job_skipped.ptr);
     pa.norm_partials = static_cast<double*>(ws->partials.ptr);
     pa.plane_counts = static_cast<unsigned long long*>(ws->plane_counts.ptr);
-    B200_TRY(mark(0));
-    B200_TRY(launch_prep(pa, dbl, opt->coord_mode, blocks, st));
-    B200_TRY(launch_finalize_prep(pa.norm_partials, (int)blocks,
-                                  pa.plane_counts, pa.support, P, counters,
-                                  d_norm, d_num_skipped, st));
-    launches += 2;
 
+    B200_TRY(mark(0));
+    if (n > 0)
+    {
+        B200_TRY(launch_prep(pa, dbl, opt->coord_mode, st));
+        launches += 1;
+    }
+    else
+    {
+        B200_TRY(cudaMemsetAsync(pa.norm_partials, 0,
+                                 sizeof(double) * num_jobs * bpj, st));
+    }
+    // Norms, skip counts and grid updates of every job (also when empty).
+    B200_TRY(launch_finalize_prep(pa, st));
+    launches += 1;
     B200_TRY(mark(1));
+    if (n == 0)
+    {
+        B200_TRY(mark(2));
+        B200_TRY(mark(3));
+        B200_TRY(mark(4));
+        ws->events_recorded = timing ? 1 : 0;
+        ws->last_launches = launches;
+        B200_TRY(cudaMemcpyAsync(ws->h_counters, counters,
+                                 sizeof(unsigned long long) * CNT_COUNT,
+                                 cudaMemcpyDeviceToHost, st));
+        return OSKAR_B200_OK;
+    }
+
     int which = 0;
     B200_TRY(radix_sort_pairs(keys, vals, n, kl.total_bits + 1,
                               ws->scan_tmp.ptr, st, &which, &launches));
     B200_TRY(mark(2));
-    B200_TRY(launch_permute(vals[which], n, counters, pa.rec, vis, weight,
-                            opt->apply_weight, dbl,
+    B200_TRY(launch_permute(vals[which], keys[which], n, counters, pa.rec,
+                            d_jobs, kl.job_shift, opt->apply_weight, dbl,
                             static_cast<int4*>(ws->srec.ptr), ws->svis.ptr,
                             ws->num_sms, st));
     launches += 1;
     B200_TRY(launch_tasks(keys[which], n, counters, 2 * kl.fine_bits,
-                          kTaskMax, static_cast<uint32_t*>(ws->flags.ptr),
+                          kl.job_shift, kTaskMax,
+                          static_cast<uint32_t*>(ws->flags.ptr),
                           keys[which ^ 1], ws->scan_tmp.ptr,
                           static_cast<uint32_t*>(ws->task_start.ptr),
+                          static_cast<uint32_t*>(ws->task_job.ptr),
                           ws->num_sms, st, &launches));
 
     GridArgs ga{};
     ga.srec = static_cast<const int4*>(ws->srec.ptr);
     ga.svis = ws->svis.ptr;
     ga.task_start = static_cast<const uint32_t*>(ws->task_start.ptr);
-    ga.planes = static_cast<const PlaneDesc*>(cube->d_planes.ptr);
-    ga.slabs = cube->d_slabs.ptr;
-    ga.grid = grid;
+    ga.task_job = static_cast<const uint32_t*>(ws->task_job.ptr);
+    ga.jobs = d_jobs;
     ga.counters = counters;
-    ga.grid_size = grid_size;
-    ga.oversample = cube->oversample;
-    ga.half = cube->half;
+    ga.comp_radius = opt->compensate_radius;
     if (opt->classes_per_thread == 1 || opt->classes_per_thread == 2 ||
         opt->classes_per_thread == 4)
         memset(ga.cpt, opt->classes_per_thread, sizeof(ga.cpt));
     else
         default_tune_table(ga.cpt);
-    // Auto staging reads the kernel slabs through L1: on plain_large it ran
-    // the gridding kernel 2.3x faster than staging each task's slab into
-    // shared memory, whose size caps residency at one CTA per SM.
-    const bool fits = grid_smem_bytes(cube, true) <= ws->smem_optin;
+    // Kernel values are read through L1 unless staging is asked for: on
+    // plain_large the L1 path is as fast as staging each row-offset run's
+    // W-row block into shared memory (24.2 ms vs 24.8 ms with FP16 slabs,
+    // 30.2 ms with FP32 slabs, whose blocks cap residency at 2 CTAs/SM).
     const bool staged = opt->staging == 1;
-    if (staged && !fits) return OSKAR_B200_ERR_UNSUPPORTED;
-    const bool comp = opt->accum_mode == OSKAR_B200_ACCUM_COMPENSATED;
-    const size_t cells = (size_t)grid_size * (size_t)grid_size;
+    if (staged && grid_smem_bytes(dbl, max_block, true) > ws->smem_optin)
+        return OSKAR_B200_ERR_UNSUPPORTED;
     if (comp)
-    {
-        // Error grid of this job: zeroed here, folded into the grid below.
-        B200_TRY(ws->comp_grid.ensure(cells * 2 * sizeof(float)));
         B200_TRY(cudaMemsetAsync(ws->comp_grid.ptr, 0,
-                                 cells * 2 * sizeof(float), st));
-        ga.comp = ws->comp_grid.ptr;
-    }
+                                 comp_floats * sizeof(float), st));
     int ctas = 0;
     B200_TRY(mark(3));
-    B200_TRY(launch_grid(ga, cube, staged, comp, ws->num_sms, st, &ctas));
+    B200_TRY(launch_grid(ga, dbl, c0->kernel_type, max_block, staged, comp,
+                         ws->num_sms, st, &ctas));
     launches += 1;
     if (comp)
     {
-        B200_TRY(launch_fold(static_cast<float*>(grid),
-                             static_cast<float*>(ws->comp_grid.ptr), cells,
-                             ws->num_sms, st));
+        B200_TRY(launch_fold_jobs(d_jobs, num_jobs, ws->num_sms, st));
         launches += 1;
     }
     B200_TRY(mark(4));
@@ -222,6 +303,54 @@ int run_grid(oskar_B200Workspace* ws, const oskar_B200Cube* cube,
                              sizeof(unsigned long long) * CNT_COUNT,
                              cudaMemcpyDeviceToHost, st));
     return OSKAR_B200_OK;
+}
+
+int run_grid(oskar_B200Workspace* ws, const oskar_B200Cube* cube,
+             const oskar_B200Options* opt, size_t n, const void* uu,
+             const void* vv, const void* ww, const void* vis,
+             const void* weight, double cell_size_rad, double w_scale,
+             int grid_size, void* grid, unsigned long long* d_num_skipped,
+             double* d_norm, cudaStream_t st)
+{
+    HostJob j{};
+    j.cube = cube;
+    j.num_points = n;
+    j.uu = uu;
+    j.vv = vv;
+    j.ww = ww;
+    j.vis = vis;
+    j.weight = weight;
+    j.cell_size_rad = cell_size_rad;
+    j.w_scale = w_scale;
+    j.grid_size = grid_size;
+    j.grid = grid;
+    j.d_num_skipped = d_num_skipped;
+    j.d_norm = d_norm;
+    return run_batch(ws, opt, 1, &j, st);
+}
+
+int run_place(oskar_B200Workspace* ws, int data_is_double, int coord_mode,
+              const int* d_support, int num_planes, int oversample,
+              size_t num_points, const void* uu, const void* vv,
+              const void* ww, double cell_size_rad, double w_scale,
+              int grid_size, int32_t* gu, int32_t* gv, int32_t* plane,
+              int32_t* off_u, int32_t* off_v, int32_t* conj,
+              int32_t* skipped, cudaStream_t st)
+{
+    PlaceConsts pc{};
+    pc.grid_scale = (double)grid_size * cell_size_rad;
+    pc.w_scale = w_scale;
+    pc.grid_scale_f = (float)grid_size * (float)cell_size_rad;
+    pc.w_scale_f = (float)w_scale;
+    pc.grid_size = grid_size;
+    pc.centre = grid_size / 2;
+    pc.num_planes = num_planes;
+    pc.oversample = oversample;
+    if (num_points == 0) return OSKAR_B200_OK;
+    return status_from_cuda(launch_place(data_is_double, coord_mode, uu, vv,
+                                         ww, num_points, pc, d_support, gu,
+                                         gv, plane, off_u, off_v, conj,
+                                         skipped, ws->num_sms, st));
 }
 
 namespace {
@@ -271,30 +400,6 @@ int measure_atomic_rate(oskar_B200Workspace* ws, void* grid, int grid_size,
     if (e != cudaSuccess) return status_from_cuda(e);
     *updates_per_s = (double)blocks * threads * iters / (ms * 1e-3);
     return OSKAR_B200_OK;
-}
-
-int run_place(oskar_B200Workspace* ws, int data_is_double, int coord_mode,
-              const int* d_support, int num_planes, int oversample,
-              size_t num_points, const void* uu, const void* vv,
-              const void* ww, double cell_size_rad, double w_scale,
-              int grid_size, int32_t* gu, int32_t* gv, int32_t* plane,
-              int32_t* off_u, int32_t* off_v, int32_t* conj,
-              int32_t* skipped, cudaStream_t st)
-{
-    PlaceConsts pc{};
-    pc.grid_scale = (double)grid_size * cell_size_rad;
-    pc.w_scale = w_scale;
-    pc.grid_scale_f = (float)grid_size * (float)cell_size_rad;
-    pc.w_scale_f = (float)w_scale;
-    pc.grid_size = grid_size;
-    pc.centre = grid_size / 2;
-    pc.num_planes = num_planes;
-    pc.oversample = oversample;
-    if (num_points == 0) return OSKAR_B200_OK;
-    return status_from_cuda(launch_place(data_is_double, coord_mode, uu, vv,
-                                         ww, num_points, pc, d_support, gu,
-                                         gv, plane, off_u, off_v, conj,
-                                         skipped, ws->num_sms, st));
 }
 
 }  // namespace b200

@@ -1,15 +1,16 @@
-// Per-visibility preparation: placement (grid cell, w-plane, oversample
-// offsets, conjugation, skip test) exactly as oskar_grid_wproj.c:70-101
-// computes it, the sort key, the skip count, the norm, the plane histogram;
-// then, after the sort, the permutation into sorted order and the gridding
-// work list (tasks).
+// Per-visibility preparation of a batch of jobs: placement (grid cell,
+// w-plane, oversample offsets, conjugation, skip test) exactly as
+// oskar_grid_wproj.c:70-101 computes it, the sort key, the skip counts, the
+// norms and the plane histograms; then, after the sort, the permutation into
+// sorted order and the gridding work list (tasks).
 #include "common.cuh"
 #include "internal.h"
 #include "prep.cuh"
 
 namespace b200 {
 
-KeyLayout make_key_layout(int grid_size, int num_planes)
+bool make_key_layout(int grid_size, int num_planes, int num_jobs,
+                     KeyLayout* out)
 {
     KeyLayout k{};
     int gbits = 0;
@@ -17,21 +18,32 @@ KeyLayout make_key_layout(int grid_size, int num_planes)
     // Coarse tiles: at most 16 per axis and at least 64 cells wide, so the
     // visibilities in flight at any time touch a few coarse tiles of grid.
     k.coarse_shift = gbits - 4 > 6 ? gbits - 4 : 6;
-    int ctiles = (grid_size + (1 << k.coarse_shift) - 1) >> k.coarse_shift;
-    k.coarse_bits = 0;
+    const int ctiles = (grid_size + (1 << k.coarse_shift) - 1) >> k.coarse_shift;
     while ((1 << k.coarse_bits) < ctiles) ++k.coarse_bits;
-    k.plane_bits = 0;
     while ((1 << k.plane_bits) < num_planes) ++k.plane_bits;
+    while ((1 << k.job_bits) < num_jobs) ++k.job_bits;
     k.fine_shift = 0;
     k.fine_bits = k.coarse_shift;
-    while (2 * k.coarse_bits + k.plane_bits + 2 * k.fine_bits + 1 > 32 &&
-           k.fine_bits > 0)
+    const int fixed = k.job_bits + 2 * k.coarse_bits + k.plane_bits + 1;
+    if (fixed > 32) return false;
+    while (fixed + 2 * k.fine_bits > 32 && k.fine_bits > 0)
     {
         ++k.fine_shift;
         --k.fine_bits;
     }
-    k.total_bits = 2 * k.coarse_bits + k.plane_bits + 2 * k.fine_bits;
-    return k;
+    k.job_shift = 2 * k.coarse_bits + k.plane_bits + 2 * k.fine_bits;
+    k.total_bits = k.job_shift + k.job_bits;
+    *out = k;
+    return true;
+}
+
+int prep_blocks_per_job(size_t max_points, int num_jobs, int num_sms)
+{
+    const size_t need = (max_points + 255) / 256;
+    size_t want = (size_t)num_sms * 8 / (size_t)(num_jobs > 0 ? num_jobs : 1);
+    if (want < 1) want = 1;
+    if (want > need) want = need > 0 ? need : 1;
+    return (int)want;
 }
 
 namespace {
@@ -50,8 +62,8 @@ __device__ __forceinline__ uint32_t spread_bits(uint32_t x)
     return x;
 }
 
-__device__ __forceinline__ uint32_t make_key(const KeyLayout& k, int gu,
-                                             int gv, int plane)
+__device__ __forceinline__ uint32_t make_key(const KeyLayout& k, int job,
+                                             int gu, int gv, int plane)
 {
     const uint32_t cu = (uint32_t)gu >> k.coarse_shift;
     const uint32_t cv = (uint32_t)gv >> k.coarse_shift;
@@ -60,62 +72,83 @@ __device__ __forceinline__ uint32_t make_key(const KeyLayout& k, int gu,
     const uint32_t fv = ((uint32_t)gv & in_mask) >> k.fine_shift;
     const uint32_t coarse = spread_bits(cu) | (spread_bits(cv) << 1);
     const uint32_t fine = spread_bits(fu) | (spread_bits(fv) << 1);
-    return (coarse << (k.plane_bits + 2 * k.fine_bits)) |
+    return ((uint32_t)job << k.job_shift) |
+           (coarse << (k.plane_bits + 2 * k.fine_bits)) |
            ((uint32_t)plane << (2 * k.fine_bits)) | fine;
+}
+
+__device__ __forceinline__ PlaceConsts place_consts(const JobDesc& jd)
+{
+    PlaceConsts pc;
+    pc.grid_scale = jd.grid_scale;
+    pc.w_scale = jd.w_scale;
+    pc.grid_scale_f = jd.grid_scale_f;
+    pc.w_scale_f = jd.w_scale_f;
+    pc.grid_size = jd.grid_size;
+    pc.centre = jd.grid_size / 2;
+    pc.num_planes = jd.num_planes;
+    pc.oversample = jd.oversample;
+    return pc;
 }
 
 template <typename T, int MODE>
 __global__ void __launch_bounds__(kPrepThreads)
 prep_kernel(const PrepArgs a)
 {
-    const T* __restrict__ uu = static_cast<const T*>(a.uu);
-    const T* __restrict__ vv = static_cast<const T*>(a.vv);
-    const T* __restrict__ ww = static_cast<const T*>(a.ww);
-    const T* __restrict__ wt = static_cast<const T*>(a.weight);
+    const int job = blockIdx.y;
+    const JobDesc& jd = a.jobs[job];
+    const T* __restrict__ uu = static_cast<const T*>(jd.uu);
+    const T* __restrict__ vv = static_cast<const T*>(jd.vv);
+    const T* __restrict__ ww = static_cast<const T*>(jd.ww);
+    const T* __restrict__ wt = static_cast<const T*>(jd.weight);
+    const PlaceConsts pc = place_consts(jd);
+    const int num_planes = jd.num_planes, half = jd.half;
+    const unsigned long long first = jd.first, n = jd.n;
     __shared__ unsigned s_hist[kMaxSmemPlanes];
     __shared__ double s_norm[kPrepThreads / 32];
     __shared__ unsigned s_skip[kPrepThreads / 32];
-    const bool smem_hist = a.num_planes <= kMaxSmemPlanes;
+    const bool smem_hist = num_planes <= kMaxSmemPlanes;
     if (smem_hist)
-        for (int p = threadIdx.x; p < a.num_planes; p += blockDim.x)
+        for (int p = threadIdx.x; p < num_planes; p += blockDim.x)
             s_hist[p] = 0;
     __syncthreads();
 
-    const int span = 2 * a.half + 1;
+    const int span = 2 * half + 1;
     const uint32_t skip_key = 1u << a.key.total_bits;
     const int lane = threadIdx.x & 31;
+    unsigned long long* job_hist = a.plane_counts + (size_t)job * a.max_planes;
     double norm = 0.0;
     unsigned skipped = 0;
     const size_t stride = (size_t)gridDim.x * blockDim.x;
-    for (size_t base = (size_t)blockIdx.x * blockDim.x; base < a.n;
+    for (size_t base = (size_t)blockIdx.x * blockDim.x; base < n;
          base += stride)
     {
         const size_t i = base + threadIdx.x;
-        const bool in_range = i < a.n;
+        const bool in_range = i < n;
+        const size_t g = first + i;
         Placed p{};
         if (in_range)
-            p = place_one<T, MODE>(uu[i], vv[i], ww[i], a.pc, a.support);
+            p = place_one<T, MODE>(uu[i], vv[i], ww[i], pc, jd.support);
         const bool keep = in_range && !p.skipped;
         if (in_range)
         {
             if (keep)
             {
-                a.rec[i] = make_int4(p.gu, p.gv,
+                a.rec[g] = make_int4(p.gu, p.gv,
                                      p.plane | (p.conj < 0 ? (int)0x80000000 : 0),
-                                     (p.off_u + a.half) |
-                                         ((p.off_v + a.half) << 16));
-                a.keys[i] = make_key(a.key, p.gu, p.gv, p.plane);
-                double s = a.norm_table[((size_t)p.plane * span +
-                                         (p.off_v + a.half)) * span +
-                                        (p.off_u + a.half)];
+                                     (p.off_u + half) | ((p.off_v + half) << 16));
+                a.keys[g] = make_key(a.key, job, p.gu, p.gv, p.plane);
+                double s = jd.norm_table[((size_t)p.plane * span +
+                                          (p.off_v + half)) * span +
+                                         (p.off_u + half)];
                 if (a.apply_weight) s *= (double)wt[i];
                 norm += s;
             }
             else
             {
-                a.keys[i] = skip_key;
+                a.keys[g] = skip_key;
             }
-            a.vals[i] = (uint32_t)i;
+            a.vals[g] = (uint32_t)g;
         }
         skipped += in_range && !keep;
         // plane histogram, aggregated across equal planes in the warp
@@ -124,7 +157,7 @@ prep_kernel(const PrepArgs a)
         if (keep && lane == __ffs(peers) - 1)
         {
             if (smem_hist) atomicAdd(&s_hist[pl], (unsigned)__popc(peers));
-            else atomicAdd(&a.plane_counts[pl], (unsigned long long)__popc(peers));
+            else atomicAdd(&job_hist[pl], (unsigned long long)__popc(peers));
         }
     }
     norm = warp_sum(norm);
@@ -144,37 +177,37 @@ prep_kernel(const PrepArgs a)
             t += s_norm[w];
             k += s_skip[w];
         }
-        a.norm_partials[blockIdx.x] = t;
-        if (k) atomicAdd(&a.counters[CNT_SKIPPED], k);
+        a.norm_partials[(size_t)job * gridDim.x + blockIdx.x] = t;
+        if (k)
+        {
+            atomicAdd(&a.job_skipped[job], k);
+            atomicAdd(&a.counters[CNT_SKIPPED], k);
+        }
     }
     if (smem_hist)
-        for (int p = threadIdx.x; p < a.num_planes; p += blockDim.x)
+        for (int p = threadIdx.x; p < num_planes; p += blockDim.x)
             if (s_hist[p])
-                atomicAdd(&a.plane_counts[p], (unsigned long long)s_hist[p]);
+                atomicAdd(&job_hist[p], (unsigned long long)s_hist[p]);
 }
 
-// Sums the per-block norm partials in a fixed order (deterministic), adds
-// them to the caller's norm, publishes the skip count, and counts grid
-// updates from the plane histogram.
-__global__ void finalize_prep_kernel(const double* __restrict__ partials,
-                                     int num_partials,
-                                     const unsigned long long* __restrict__ plane_counts,
-                                     const int* __restrict__ support,
-                                     int num_planes,
-                                     unsigned long long* __restrict__ counters,
-                                     double* __restrict__ d_norm,
-                                     unsigned long long* __restrict__ d_skipped)
+// One block per job: sums the job's norm partials in a fixed order
+// (deterministic), adds them to the caller's norm, publishes the skip count,
+// and counts grid updates from the plane histogram.
+__global__ void finalize_prep_kernel(const PrepArgs a)
 {
+    const int job = blockIdx.x;
+    const JobDesc& jd = a.jobs[job];
     __shared__ double s_v[32];
     __shared__ unsigned long long s_u[32];
     double t = 0.0;
-    for (int i = threadIdx.x; i < num_partials; i += blockDim.x)
-        t += partials[i];
+    for (int i = threadIdx.x; i < a.blocks_per_job; i += blockDim.x)
+        t += a.norm_partials[(size_t)job * a.blocks_per_job + i];
     unsigned long long up = 0;
-    for (int p = threadIdx.x; p < num_planes; p += blockDim.x)
+    const unsigned long long* hist = a.plane_counts + (size_t)job * a.max_planes;
+    for (int p = threadIdx.x; p < jd.num_planes; p += blockDim.x)
     {
-        const unsigned long long w = 2ull * support[p] + 1ull;
-        up += plane_counts[p] * w * w;
+        const unsigned long long w = 2ull * jd.support[p] + 1ull;
+        up += hist[p] * w * w;
     }
     t = warp_sum(t);
     up = warp_sum(up);
@@ -193,30 +226,35 @@ __global__ void finalize_prep_kernel(const double* __restrict__ partials,
             s += s_v[w];
             u += s_u[w];
         }
-        if (d_norm) *d_norm += s;
-        if (d_skipped) *d_skipped = counters[CNT_SKIPPED];
-        counters[CNT_UPDATES] = u;
+        if (jd.d_norm) *jd.d_norm += s;
+        if (jd.d_skipped) *jd.d_skipped = a.job_skipped[job];
+        atomicAdd(&a.counters[CNT_UPDATES], u);
     }
 }
 
 template <typename T>
-__global__ void permute_kernel(const uint32_t* __restrict__ order, size_t n,
+__global__ void permute_kernel(const uint32_t* __restrict__ order,
+                               const uint32_t* __restrict__ sorted_keys,
+                               size_t n,
                                const unsigned long long* __restrict__ counters,
                                const int4* __restrict__ rec,
-                               const T* __restrict__ vis,
-                               const T* __restrict__ weight, int apply_weight,
-                               int4* __restrict__ srec, T* __restrict__ svis)
+                               const JobDesc* __restrict__ jobs, int job_shift,
+                               int apply_weight, int4* __restrict__ srec,
+                               T* __restrict__ svis)
 {
     const size_t valid = n - counters[CNT_SKIPPED];
     for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < valid;
          s += (size_t)gridDim.x * blockDim.x)
     {
         const uint32_t i = order[s];
+        const JobDesc& jd = jobs[sorted_keys[s] >> job_shift];
+        const size_t local = i - jd.first;
+        const T* vis = static_cast<const T*>(jd.vis);
         srec[s] = rec[i];
-        T re = vis[2 * (size_t)i], im = vis[2 * (size_t)i + 1];
+        T re = vis[2 * local], im = vis[2 * local + 1];
         if (apply_weight)
         {
-            const T w = weight[i];
+            const T w = static_cast<const T*>(jd.weight)[local];
             re *= w;
             im *= w;
         }
@@ -225,8 +263,6 @@ __global__ void permute_kernel(const uint32_t* __restrict__ order, size_t n,
     }
 }
 
-// Task boundaries: a new task starts where the (coarse tile, plane) part of
-// the sorted key changes, and every task_max positions.
 __global__ void task_flags_kernel(const uint32_t* __restrict__ keys, size_t n,
                                   const unsigned long long* __restrict__ counters,
                                   int fine_key_bits, int task_max,
@@ -247,14 +283,21 @@ __global__ void task_flags_kernel(const uint32_t* __restrict__ keys, size_t n,
 }
 
 __global__ void task_scatter_kernel(const uint32_t* __restrict__ flags,
-                                    const uint32_t* __restrict__ pos, size_t n,
+                                    const uint32_t* __restrict__ pos,
+                                    const uint32_t* __restrict__ keys, size_t n,
+                                    int job_shift,
                                     unsigned long long* __restrict__ counters,
-                                    uint32_t* __restrict__ task_start)
+                                    uint32_t* __restrict__ task_start,
+                                    uint32_t* __restrict__ task_job)
 {
     for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < n;
          s += (size_t)gridDim.x * blockDim.x)
     {
-        if (flags[s]) task_start[pos[s]] = (uint32_t)s;
+        if (flags[s])
+        {
+            task_start[pos[s]] = (uint32_t)s;
+            task_job[pos[s]] = keys[s] >> job_shift;
+        }
         if (s == n - 1)
         {
             const uint32_t num_tasks = pos[s] + flags[s];
@@ -296,60 +339,49 @@ unsigned grid_blocks(size_t n, int num_sms, int per_sm, int threads)
 
 }  // namespace
 
-unsigned prep_num_blocks(size_t n, int num_sms)
-{
-    return grid_blocks(n, num_sms, 8, kPrepThreads);
-}
-
 cudaError_t launch_prep(const PrepArgs& a, int data_is_double, int coord_mode,
-                        unsigned blocks, cudaStream_t st)
+                        cudaStream_t st)
 {
+    const dim3 grid(a.blocks_per_job, a.num_jobs);
     if (data_is_double)
-        prep_kernel<double, COORD_F64><<<blocks, kPrepThreads, 0, st>>>(a);
+        prep_kernel<double, COORD_F64><<<grid, kPrepThreads, 0, st>>>(a);
     else if (coord_mode == OSKAR_B200_COORDS_REFERENCE_F32)
-        prep_kernel<float, COORD_REF_F32><<<blocks, kPrepThreads, 0, st>>>(a);
+        prep_kernel<float, COORD_REF_F32><<<grid, kPrepThreads, 0, st>>>(a);
     else
-        prep_kernel<float, COORD_F64><<<blocks, kPrepThreads, 0, st>>>(a);
+        prep_kernel<float, COORD_F64><<<grid, kPrepThreads, 0, st>>>(a);
     return cudaGetLastError();
 }
 
-cudaError_t launch_finalize_prep(const double* partials, int num_partials,
-                                 const unsigned long long* plane_counts,
-                                 const int* support, int num_planes,
-                                 unsigned long long* counters, double* d_norm,
-                                 unsigned long long* d_skipped, cudaStream_t st)
+cudaError_t launch_finalize_prep(const PrepArgs& a, cudaStream_t st)
 {
-    finalize_prep_kernel<<<1, 1024, 0, st>>>(partials, num_partials,
-                                             plane_counts, support, num_planes,
-                                             counters, d_norm, d_skipped);
+    finalize_prep_kernel<<<a.num_jobs, 256, 0, st>>>(a);
     return cudaGetLastError();
 }
 
-cudaError_t launch_permute(const uint32_t* order, size_t n,
-                           const unsigned long long* counters, const int4* rec,
-                           const void* vis, const void* weight,
+cudaError_t launch_permute(const uint32_t* order, const uint32_t* sorted_keys,
+                           size_t n, const unsigned long long* counters,
+                           const int4* rec, const JobDesc* jobs, int job_shift,
                            int apply_weight, int data_is_double, int4* srec,
                            void* svis, int num_sms, cudaStream_t st)
 {
     const unsigned blocks = grid_blocks(n, num_sms, 8, 256);
     if (data_is_double)
         permute_kernel<double><<<blocks, 256, 0, st>>>(
-            order, n, counters, rec, static_cast<const double*>(vis),
-            static_cast<const double*>(weight), apply_weight, srec,
-            static_cast<double*>(svis));
+            order, sorted_keys, n, counters, rec, jobs, job_shift,
+            apply_weight, srec, static_cast<double*>(svis));
     else
         permute_kernel<float><<<blocks, 256, 0, st>>>(
-            order, n, counters, rec, static_cast<const float*>(vis),
-            static_cast<const float*>(weight), apply_weight, srec,
-            static_cast<float*>(svis));
+            order, sorted_keys, n, counters, rec, jobs, job_shift,
+            apply_weight, srec, static_cast<float*>(svis));
     return cudaGetLastError();
 }
 
 cudaError_t launch_tasks(const uint32_t* sorted_keys, size_t n,
                          unsigned long long* counters, int fine_key_bits,
-                         int task_max, uint32_t* flags, uint32_t* pos,
-                         void* scan_tmp, uint32_t* task_start, int num_sms,
-                         cudaStream_t st, int* launches)
+                         int job_shift, int task_max, uint32_t* flags,
+                         uint32_t* pos, void* scan_tmp, uint32_t* task_start,
+                         uint32_t* task_job, int num_sms, cudaStream_t st,
+                         int* launches)
 {
     const unsigned blocks = grid_blocks(n, num_sms, 8, 256);
     task_flags_kernel<<<blocks, 256, 0, st>>>(sorted_keys, n, counters,
@@ -357,8 +389,9 @@ cudaError_t launch_tasks(const uint32_t* sorted_keys, size_t n,
     cudaError_t e = exclusive_scan_u32(flags, pos, n, scan_tmp, st, launches);
     if (e != cudaSuccess) return e;
     if (launches) *launches += 2;
-    task_scatter_kernel<<<blocks, 256, 0, st>>>(flags, pos, n, counters,
-                                                task_start);
+    task_scatter_kernel<<<blocks, 256, 0, st>>>(flags, pos, sorted_keys, n,
+                                                job_shift, counters,
+                                                task_start, task_job);
     return cudaGetLastError();
 }
 

@@ -101,46 +101,46 @@ __device__ __forceinline__ Placed place_one(T u, T v, T w,
     return p;
 }
 
+// Prep of a batch: launch grid (blocks_per_job, num_jobs), block (x, j)
+// walks job j's points.
 struct PrepArgs
 {
-    const void* uu;
-    const void* vv;
-    const void* ww;
-    const void* weight;
-    size_t n;
-    PlaceConsts pc;
-    const int* support;
-    int num_planes;
-    int half;
+    const JobDesc* jobs;
+    int num_jobs;
+    int blocks_per_job;
+    int max_planes;          // row stride of plane_counts
     int apply_weight;
-    const double* norm_table;
     KeyLayout key;
-    int4* rec;
+    int4* rec;               // [total points], global index
     uint32_t* keys;
     uint32_t* vals;
-    unsigned long long* counters;
-    double* norm_partials;
-    unsigned long long* plane_counts;
+    unsigned long long* counters;     // CNT_SKIPPED: all jobs
+    unsigned long long* job_skipped;  // [num_jobs]
+    double* norm_partials;            // [num_jobs][blocks_per_job]
+    unsigned long long* plane_counts; // [num_jobs][max_planes]
 };
 
-unsigned prep_num_blocks(size_t n, int num_sms);
+// Blocks per job: about 8 per SM over the whole batch, at least one per job,
+// no more than the largest job needs.
+int prep_blocks_per_job(size_t max_points, int num_jobs, int num_sms);
 cudaError_t launch_prep(const PrepArgs& a, int data_is_double, int coord_mode,
-                        unsigned blocks, cudaStream_t st);
-cudaError_t launch_finalize_prep(const double* partials, int num_partials,
-                                 const unsigned long long* plane_counts,
-                                 const int* support, int num_planes,
-                                 unsigned long long* counters, double* d_norm,
-                                 unsigned long long* d_skipped, cudaStream_t st);
-cudaError_t launch_permute(const uint32_t* order, size_t n,
-                           const unsigned long long* counters, const int4* rec,
-                           const void* vis, const void* weight,
+                        cudaStream_t st);
+// Per job: norm += sum of its partials; skip count; grid updates.
+cudaError_t launch_finalize_prep(const PrepArgs& a, cudaStream_t st);
+// srec[s] = rec[order[s]], svis[s] = vis of that point (x weight).
+cudaError_t launch_permute(const uint32_t* order, const uint32_t* sorted_keys,
+                           size_t n, const unsigned long long* counters,
+                           const int4* rec, const JobDesc* jobs, int job_shift,
                            int apply_weight, int data_is_double, int4* srec,
                            void* svis, int num_sms, cudaStream_t st);
+// Task list: a task starts where (job, coarse tile, plane) changes and every
+// task_max positions; task_job[t] is the job of task t.
 cudaError_t launch_tasks(const uint32_t* sorted_keys, size_t n,
                          unsigned long long* counters, int fine_key_bits,
-                         int task_max, uint32_t* flags, uint32_t* pos,
-                         void* scan_tmp, uint32_t* task_start, int num_sms,
-                         cudaStream_t st, int* launches);
+                         int job_shift, int task_max, uint32_t* flags,
+                         uint32_t* pos, void* scan_tmp, uint32_t* task_start,
+                         uint32_t* task_job, int num_sms, cudaStream_t st,
+                         int* launches);
 cudaError_t launch_place(int data_is_double, int coord_mode, const void* uu,
                          const void* vv, const void* ww, size_t n,
                          const PlaceConsts& pc, const int* support,

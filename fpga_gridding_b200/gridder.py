@@ -207,6 +207,33 @@ def grid_device(ws: Workspace, cube: Cube, uu, vv, ww, vis, weight,
         _ptr(d_norm), _stream_ptr(stream)), "oskar_b200_grid")
 
 
+def grid_batch_device(ws: Workspace, jobs, opts: Options | None = None,
+                      stream=None) -> None:
+    """Asynchronous batched gridding.  `jobs` is a sequence of dicts with
+    the keys of grid_device: cube, uu, vv, ww, vis, weight, cell_size_rad,
+    w_scale, grid_size, grid and optionally d_num_skipped, d_norm (device
+    tensors).  One sort and one persistent gridding launch serve all jobs."""
+    lib = load()
+    if opts is None:
+        opts = options()
+    arr = (_lib.Job * len(jobs))()
+    keep = []
+    for i, j in enumerate(jobs):
+        arr[i].cube = j["cube"].handle
+        arr[i].num_points = j["uu"].numel()
+        for k in ("uu", "vv", "ww", "vis", "weight", "grid", "d_num_skipped",
+                  "d_norm"):
+            t = j.get(k)
+            setattr(arr[i], k, t.data_ptr() if t is not None else None)
+            keep.append(t)
+        arr[i].cell_size_rad = float(j["cell_size_rad"])
+        arr[i].w_scale = float(j["w_scale"])
+        arr[i].grid_size = int(j["grid_size"])
+    check(lib.oskar_b200_grid_batch(ws.handle, C.byref(opts), len(jobs), arr,
+                                    _stream_ptr(stream)),
+          "oskar_b200_grid_batch")
+
+
 def place_device(ws: Workspace, support, oversample: int, uu, vv, ww,
                  cell_size_rad: float, w_scale: float, grid_size: int,
                  coord_mode: int = _lib.COORDS_F64, stream=None) -> dict:

@@ -181,17 +181,20 @@ def analytic_kernel_cube(support: np.ndarray, oversample: int,
     num_planes = len(support)
     idx = torch.arange(conv_size_half, dtype=torch.float64, device=device)
     r2 = (idx[None, :] ** 2 + idx[:, None] ** 2) / float(oversample) ** 2
-    cube = torch.empty(num_planes, conv_size_half, conv_size_half, 2,
-                       dtype=torch.float64, device=device)
-    for p in range(num_planes):
-        s = int(support[p])
-        sigma = s / taper_div
-        taper = torch.exp(-r2 / (2 * sigma * sigma))
-        taps = torch.arange(-s, s + 1, device=device).abs() * oversample
-        norm = taper[taps][:, taps].sum()
-        phase = 2 * math.pi * chirp * p * r2
-        cube[p, :, :, 0] = taper * torch.cos(phase) / norm
-        cube[p, :, :, 1] = taper * torch.sin(phase) / norm
+    s = torch.as_tensor(np.asarray(support, dtype=np.float64), device=device)
+    sigma = s / taper_div
+    taper = torch.exp(-r2[None] / (2 * (sigma * sigma)[:, None, None]))
+    # zero-offset taps k = -S..S read quadrant index |k| * os: index 0 once,
+    # k * os (k = 1..S) twice
+    k = torch.arange(conv_size_half, device=device)
+    on_tap = (k[None, :] % oversample == 0) & \
+        (k[None, :] <= (s[:, None] * oversample))
+    mult = on_tap.double() * torch.where(k[None, :] == 0, 1.0, 2.0)
+    norm = torch.einsum("pi,pij,pj->p", mult, taper, mult)
+    p = torch.arange(num_planes, dtype=torch.float64, device=device)
+    phase = 2 * math.pi * chirp * p[:, None, None] * r2[None]
+    cube = torch.stack([taper * torch.cos(phase), taper * torch.sin(phase)],
+                       dim=-1) / norm[:, None, None, None]
     return cube.reshape(-1)
 
 
@@ -257,6 +260,117 @@ def plain_large(seed: int = 1, device="cpu", num_stations=512, num_times=300,
     csh = 37 * oversample + 1
     return _finish("plain_large", uu, vv, ww, vis, support, oversample, csh,
                    cell, w_scale, grid_size, gen, device, seed=seed)
+
+
+def batch_channels(seed: int = 2, device="cpu", num_channels=128,
+                   num_stations=256, num_times=60, grid_size=2048,
+                   num_w_planes=64, f_lo=50e6, f_hi=350e6, max_flag=0.7,
+                   s_lo=3, s_hi=24, oversample=4) -> list:
+    """Batching workload: num_channels channels spanning f_lo..f_hi, each
+    gridded into its own grid with its own kernel cube.  Array: 256 stations
+    uniform in a disk 10 km across (5 km radius), 60 samples 10 s apart, dec
+    -30 deg (32,640 baselines, 1,958,400 visibilities per channel before
+    flagging).  Seeded random flagging removes a U(0, max_flag) fraction of
+    each channel.  Per channel: num_w_planes planes with support ramping from
+    s_lo to s_lo + (s_hi - s_lo) * f / f_hi (scaled by frequency), w_scale =
+    (P-1)^2 / max|w|, oversample 4.  One cell size for all channels, chosen
+    so the highest channel's longest baseline plus its support fits.
+    Returns a list of Workloads (FP64; convert with .to)."""
+    gen = torch.Generator().manual_seed(seed)
+    enu = stations_uniform_disk(num_stations, 5000.0, gen)
+    lat = dec = math.radians(-30.0)
+    bxyz = baselines_xyz(enu, lat)
+    # uvw in metres (scale 1 Hz -> multiply by f / c per channel)
+    um, vm, wm = earth_rotation_uvw(bxyz, num_times, 10.0, C_LIGHT, dec,
+                                    device)
+    freqs = torch.linspace(f_lo, f_hi, num_channels, dtype=torch.float64)
+    uv_max_hi = float(torch.maximum(um.abs().max(), vm.abs().max())) * \
+        f_hi / C_LIGHT
+    cell = (grid_size // 2 - s_hi - 2) / (grid_size * uv_max_hi)
+    out = []
+    n_all = um.numel()
+    for ch in range(num_channels):
+        f = float(freqs[ch])
+        scale = f / C_LIGHT
+        keep_frac = 1.0 - max_flag * float(torch.rand(1, generator=gen))
+        flags = torch.rand(n_all, generator=gen) < keep_frac
+        idx = torch.nonzero(flags).squeeze(1).to(device)
+        uu, vv, ww = um[idx] * scale, vm[idx] * scale, wm[idx] * scale
+        vis = point_source_vis(uu, vv, ww, 10, math.radians(1.0), 0.1, gen)
+        s_max = int(round(s_lo + (s_hi - s_lo) * f / f_hi))
+        support = support_ramp(num_w_planes, s_lo, s_max)
+        w_scale = float((num_w_planes - 1) ** 2 / ww.abs().max().item())
+        csh = min_conv_size_half(support, oversample) + 1
+        out.append(_finish(f"channel_{ch}", uu, vv, ww, vis, support,
+                           oversample, csh, cell, w_scale, grid_size, gen,
+                           device, seed=seed, channel=ch, freq_hz=f,
+                           kept=keep_frac))
+    return out
+
+
+def serving_stream(num_jobs: int = 2000, seed: int = 4, device="cpu",
+                   n_lo: float = 1e4, n_hi: float = 5e7,
+                   grid_sizes=(512, 1024, 2048, 4096, 8192),
+                   p_lo: int = 8, p_hi: int = 256, s_lo: int = 3,
+                   s_hi: int = 32, shared_frac: float = 0.2,
+                   num_shared: int = 8, num_stations: int = 512,
+                   oversample: int = 4):
+    """Serving workload: num_jobs gridding jobs whose visibility counts are
+    log-uniform in [n_lo, n_hi], grid sizes drawn from grid_sizes, 8-256
+    w-planes and a largest support of 3-32 (support ramps from 3); about
+    shared_frac of the jobs use one of num_shared shared kernel-cube specs,
+    the rest their own.  Every job is a contiguous slice of one base
+    observation (plain_large's array: 512 stations log-radial to 30 km,
+    150 MHz, 10 s samples, enough samples for n_hi visibilities), with the
+    cell and w_scale chosen for that slice so nothing is skipped.
+    Returns (base, jobs): base holds FP32 device tensors uu, vv, ww, vis,
+    weight; each job is a dict with start, n, grid_size, cell_size_rad,
+    w_scale, cube_key; cube specs are in cubes[cube_key] = (support,
+    conv_size_half)."""
+    rng = np.random.default_rng(seed)
+    gen = torch.Generator().manual_seed(seed)
+    enu = stations_log_radial(num_stations, 20.0, 30000.0, gen)
+    nb = num_stations * (num_stations - 1) // 2
+    num_times = int(math.ceil(n_hi / nb))
+    lat = dec = math.radians(-30.0)
+    uu, vv, ww = earth_rotation_uvw(baselines_xyz(enu, lat), num_times, 10.0,
+                                    150e6, dec, device)
+    vis = point_source_vis(uu, vv, ww, 10, math.radians(1.0), 0.1, gen)
+    base = dict(uu=uu.float(), vv=vv.float(), ww=ww.float(), vis=vis.float(),
+                weight=torch.ones_like(uu, dtype=torch.float32))
+    total = uu.numel()
+
+    def spec():
+        p = int(rng.integers(p_lo, p_hi + 1))
+        s = int(rng.integers(s_lo, s_hi + 1))
+        sup = support_ramp(p, s_lo, s)
+        return sup, min_conv_size_half(sup, oversample) + 1
+
+    cubes = {}
+    for k in range(num_shared):
+        cubes[("shared", k)] = spec()
+    jobs = []
+    absu = torch.maximum(uu.abs(), vv.abs())
+    absw = ww.abs()
+    for j in range(num_jobs):
+        n = int(round(math.exp(rng.uniform(math.log(n_lo), math.log(n_hi)))))
+        n = min(n, total)
+        start = int(rng.integers(0, total - n + 1))
+        g = int(rng.choice(grid_sizes))
+        if rng.uniform() < shared_frac:
+            key = ("shared", int(rng.integers(0, num_shared)))
+        else:
+            key = ("job", j)
+            cubes[key] = spec()
+        sup, csh = cubes[key]
+        uv_max = float(absu[start:start + n].max())
+        w_max = float(absw[start:start + n].max())
+        cell = (g // 2 - int(sup.max()) - 2) / (g * uv_max)
+        w_scale = (len(sup) - 1) ** 2 / w_max if w_max > 0 else 1.0
+        jobs.append(dict(start=start, n=n, grid_size=g,
+                         cell_size_rad=float(np.float32(cell)),
+                         w_scale=float(np.float32(w_scale)), cube_key=key))
+    return base, jobs, cubes
 
 
 def scaled(workload_fn, **overrides):

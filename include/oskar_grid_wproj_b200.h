@@ -150,7 +150,11 @@ typedef struct oskar_B200Options
     int apply_weight;    /* 0: ignore weight (reference); 1: vis and norm x weight */
     int classes_per_thread; /* 0: autotuned table; 1, 2 or 4 forces it */
     int staging;         /* 0: auto; 1: TMA bulk copy to shared; 2: L1 reads */
-    int reserved[10];
+    int compensate_radius; /* ACCUM_COMPENSATED: compensate only work whose
+                            * footprint centre lies within this many cells of
+                            * the grid centre (the heavily hit cells);
+                            * 0: everywhere */
+    int reserved[9];
 } oskar_B200Options;
 
 /* Fills the defaults (FP64 coordinates, native kernels, plain accumulation,
@@ -199,6 +203,36 @@ OSKAR_B200_EXPORT int oskar_b200_grid(oskar_B200Workspace* ws,
         double w_scale, int grid_size, void* grid,
         unsigned long long* d_num_skipped, double* d_norm, void* stream);
 
+/* One job of a batch: the arguments of oskar_b200_grid. */
+typedef struct oskar_B200Job
+{
+    const oskar_B200Cube* cube;
+    size_t num_points;
+    const void* uu;
+    const void* vv;
+    const void* ww;
+    const void* vis;
+    const void* weight;
+    double cell_size_rad;
+    double w_scale;
+    int grid_size;
+    void* grid;
+    unsigned long long* d_num_skipped;
+    double* d_norm;
+} oskar_B200Job;
+
+/* Grids many independent jobs (channels, snapshots) with uneven sizes and
+ * their own cubes and grids in one pipeline: one sort over all
+ * visibilities and one persistent gridding launch that takes work from a
+ * device queue spanning every job.  All cubes must share the data precision
+ * and storage type.  Each job's result equals oskar_b200_grid on that job
+ * alone (up to floating-point summation order).  The call only enqueues
+ * device work on `stream`, so it can be captured into a CUDA graph once its
+ * buffers have been sized by an earlier call with the same jobs. */
+OSKAR_B200_EXPORT int oskar_b200_grid_batch(oskar_B200Workspace* ws,
+        const oskar_B200Options* opt, int num_jobs, const oskar_B200Job* jobs,
+        void* stream);
+
 /* Per-visibility placement exactly as the gridder computes it (device
  * pointers, int32 outputs, any may be NULL): grid cell, clamped w-plane,
  * oversample offsets, conjugation sign (+1/-1) and skip flag (0/1). */
@@ -242,6 +276,69 @@ OSKAR_B200_EXPORT int oskar_b200_set_stage_timing(oskar_B200Workspace* ws,
  * complex updates per second in *updates_per_s. */
 OSKAR_B200_EXPORT int oskar_b200_measure_atomic_rate(oskar_B200Workspace* ws,
         void* grid, int grid_size, int iters, double* updates_per_s);
+
+/* ---------------------------------------------------------------------- */
+/* 3. Serving                                                             */
+/* ---------------------------------------------------------------------- */
+
+/* A resident gridding server on one device.  A server thread admits
+ * submitted jobs in arrival order as slots and memory free up: each of
+ * `num_slots` slots owns a workspace and a stream, so admitted jobs run
+ * concurrently on the device; queued jobs that fit together are merged into
+ * one batched launch (continuous batching).  The server owns each job's
+ * output grid, allocated (zeroed) at admission; the HBM budget covers the
+ * slots' workspaces and the live output grids, and a job waits until it
+ * fits.  Cubes and input visibilities stay the caller's (device memory). */
+typedef struct oskar_B200Server oskar_B200Server;
+
+typedef struct oskar_B200Request
+{
+    unsigned long long tag;        /* caller's id, echoed in the completion */
+    const oskar_B200Cube* cube;    /* resident, may be shared by requests */
+    size_t num_points;
+    const void* uu;                /* device pointers, cube's precision */
+    const void* vv;
+    const void* ww;
+    const void* vis;
+    const void* weight;
+    double cell_size_rad;
+    double w_scale;
+    int grid_size;
+} oskar_B200Request;
+
+typedef struct oskar_B200Completion
+{
+    unsigned long long tag;
+    int status;                    /* oskar_B200Status of the job */
+    unsigned long long num_skipped;
+    double norm;
+    void* grid;                    /* device grid owned by the server until
+                                      oskar_b200_server_release(tag) */
+    double submit_s, start_s, end_s;   /* server clock (oskar_b200_server_clock) */
+    int batch_size;                /* jobs in the launch that ran it */
+} oskar_B200Completion;
+
+OSKAR_B200_EXPORT int oskar_b200_server_create(int device,
+        size_t hbm_budget_bytes, int num_slots, int max_batch_jobs,
+        const oskar_B200Options* opt, oskar_B200Server** server);
+/* Queues a job (non-blocking). */
+OSKAR_B200_EXPORT int oskar_b200_server_submit(oskar_B200Server* server,
+        const oskar_B200Request* request);
+/* Returns up to max_out completed jobs, waiting up to timeout_s for the
+ * first one; *num_out may be 0 on timeout. */
+OSKAR_B200_EXPORT int oskar_b200_server_poll(oskar_B200Server* server,
+        oskar_B200Completion* out, int max_out, int* num_out,
+        double timeout_s);
+/* Returns a completed job's grid to the server (and its budget). */
+OSKAR_B200_EXPORT int oskar_b200_server_release(oskar_B200Server* server,
+        unsigned long long tag);
+/* Seconds since the server started (the clock of the completions). */
+OSKAR_B200_EXPORT double oskar_b200_server_clock(oskar_B200Server* server);
+/* Device bytes the server holds now, and its budget. */
+OSKAR_B200_EXPORT int oskar_b200_server_memory(oskar_B200Server* server,
+        size_t* bytes_in_use, size_t* budget);
+/* Drains all jobs, frees every grid and workspace, stops the thread. */
+OSKAR_B200_EXPORT int oskar_b200_server_free(oskar_B200Server* server);
 
 /* Library build description (arch, version). */
 OSKAR_B200_EXPORT const char* oskar_b200_build_info(void);
