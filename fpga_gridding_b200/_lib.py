@@ -29,6 +29,7 @@ EXPORTED_SYMBOLS = (
     "oskar_b200_last_stats",
     "oskar_b200_set_stage_timing",
     "oskar_b200_measure_atomic_rate",
+    "oskar_b200_grid_f_static",
     "oskar_b200_server_create",
     "oskar_b200_server_submit",
     "oskar_b200_server_poll",
@@ -151,6 +152,10 @@ def load():
         _P, _P, C.c_int, C.c_int, C.POINTER(C.c_double)]
     lib.oskar_b200_grid_batch.argtypes = [_P, C.POINTER(Options), C.c_int,
                                           C.POINTER(Job), _P]
+    lib.oskar_b200_grid_f_static.argtypes = [
+        _SZ, _P, C.c_int, C.c_int, _P, _SZ, _P, _P, _P, _P, C.c_float,
+        C.c_float, C.c_int, _P, _P, _P, _P]
+    lib.oskar_b200_grid_f_static.restype = C.c_int
     lib.oskar_b200_server_create.argtypes = [C.c_int, _SZ, C.c_int, C.c_int,
                                              C.POINTER(Options),
                                              C.POINTER(_P)]

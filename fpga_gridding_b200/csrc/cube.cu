@@ -263,4 +263,53 @@ int cube_build(oskar_B200Cube* c, const void* d_conv, int conv_is_double,
     return status_from_cuda(cudaGetLastError());
 }
 
+// Host-side slab geometry of an FP32 cube (the same layout cube_build
+// gives), for callers that place the re-laid cube in memory they provide.
+size_t static_cube_geometry(int num_planes, const int* support,
+                            int oversample, std::vector<PlaneDesc>* planes,
+                            unsigned* max_block_bytes)
+{
+    const int half = (oversample + 1) / 2;
+    const int elem = (int)sizeof(float2);
+    long long off = 0;
+    unsigned max_block = 0;
+    planes->assign((size_t)num_planes, PlaneDesc{});
+    for (int p = 0; p < num_planes; ++p)
+    {
+        PlaneDesc& d = (*planes)[p];
+        d.support = support[p];
+        d.extent = oversample * d.support + half + 1;
+        d.L = (d.extent + oversample - 1) / oversample;
+        d.pitch = (oversample * d.L + 3) / 4 * 4;
+        d.rows = (2 * half + 1) * (2 * d.support + 1);
+        const unsigned block = (unsigned)((2 * d.support + 1) * d.pitch * elem);
+        if (block > max_block) max_block = block;
+        d.offset = off;
+        const size_t elems = ((size_t)d.rows * d.pitch + 1) / 2 * 2;
+        d.bytes = (unsigned)(elems * elem);
+        d.scale = 1.0f;
+        off += (long long)elems;
+    }
+    *max_block_bytes = max_block;
+    return (size_t)off * elem;
+}
+
+// Re-lays an FP32 cube (device, reference layout) into d_slabs and fills
+// the norm table, using only the memory given: d_planes must already hold
+// `planes` (see static_cube_geometry).
+int static_cube_fill(const float* d_conv, int num_planes, int oversample,
+                     int conv_size_half, const PlaneDesc* d_planes,
+                     float2* d_slabs, double* d_norm_table, cudaStream_t st)
+{
+    const int half = (oversample + 1) / 2;
+    relayout_kernel<float, float2><<<dim3(64, num_planes), 256, 0, st>>>(
+        d_conv, d_planes, oversample, half, conv_size_half, d_slabs);
+    const int span = 2 * half + 1;
+    const int entries = num_planes * span * span;
+    norm_table_kernel<float><<<(entries + 127) / 128, 128, 0, st>>>(
+        d_conv, d_planes, num_planes, oversample, half, conv_size_half,
+        d_norm_table);
+    return status_from_cuda(cudaGetLastError());
+}
+
 }  // namespace b200

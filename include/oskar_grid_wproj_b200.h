@@ -277,6 +277,34 @@ OSKAR_B200_EXPORT int oskar_b200_set_stage_timing(oskar_B200Workspace* ws,
 OSKAR_B200_EXPORT int oskar_b200_measure_atomic_rate(oskar_B200Workspace* ws,
         void* grid, int grid_size, int iters, double* updates_per_s);
 
+/* Gridding that allocates no device memory.  No counterpart in the
+ * reference (whose CPU gridder needs no device memory at all).
+ *
+ * For callers that must not call cudaMalloc: code running inside a memory
+ * pool fixed up front, a service whose device memory is provisioned by an
+ * operator or scheduler, or a thread that must not take the allocator's
+ * locks or risk its implicit device synchronisation while other streams
+ * run.  Grids one FP32 job (FP64 placement, as oskar_grid_wproj_f) into
+ * `grid` (device, accumulates), adding to *d_norm and writing
+ * *d_num_skipped (device, either may be NULL).  conv_func, uu, vv, ww, vis
+ * are device pointers; support is host memory; weight is ignored as in the
+ * reference.  All scratch (the re-laid cube, sort keys, records, task list)
+ * comes from one static device array of 64 MiB that every GPU loading this
+ * library holds until the process exits: enough for about 850,000
+ * visibilities with a small cube.  A job that does not fit returns
+ * OSKAR_B200_ERR_OVER_BUDGET and touches nothing.  The array's device
+ * address is looked up on the first call on each device (with that device
+ * current), so make that first call outside any stream capture.  Every call
+ * shares the array: calls whose device work can overlap (other streams,
+ * other threads) race and must be serialised by the caller.  Asynchronous on
+ * `stream` (NULL: the legacy default stream). */
+OSKAR_B200_EXPORT int oskar_b200_grid_f_static(size_t num_w_planes,
+        const int* support, int oversample, int conv_size_half,
+        const float* conv_func, size_t num_points, const float* uu,
+        const float* vv, const float* ww, const float* vis,
+        float cell_size_rad, float w_scale, int grid_size, float* grid,
+        unsigned long long* d_num_skipped, double* d_norm, void* stream);
+
 /* ---------------------------------------------------------------------- */
 /* 3. Serving                                                             */
 /* ---------------------------------------------------------------------- */
