@@ -446,8 +446,8 @@ BATCH_DESC = ("batch128: 128 channels 50-350 MHz, each into its own 2048^2 "
 
 def run_batch128(args, world, rank, local):
     """Batched gridding of 128 uneven channels in one graph-captured
-    pipeline (FP16 kernels, compensated FP32 accumulation) against the same
-    channels as 128 sequential plain FP32 jobs."""
+    pipeline (FP32) against the same channels as 128 sequential FP32 jobs;
+    the FP16-kernel compensated batch is timed beside it."""
     import ctypes as C
     import fpga_gridding_b200 as fg
     from fpga_gridding_b200 import _lib, workloads as W
@@ -503,7 +503,8 @@ def run_batch128(args, world, rank, local):
                            j["d_norm"], opts=plain, stream=s)
     seq_ms = timed(sequential)
 
-    # (b) one batch, FP32 plain (same arithmetic as (a)), graph-captured
+    # (b) one batch, FP32 plain (the same arithmetic as (a)), captured in a
+    # CUDA graph: the headline
     def graph_of(jobs, opts):
         fg.grid_batch_device(ws, jobs, opts=opts, stream=s)  # sizes buffers
         s.synchronize()
@@ -511,57 +512,81 @@ def run_batch128(args, world, rank, local):
         with torch.cuda.graph(g, stream=s):
             fg.grid_batch_device(ws, jobs, opts=opts, stream=s)
         return g
+
+    def replay_on_s(g):
+        # torch launches a replay on the current stream; keep every use of
+        # the workspace's buffers on s.
+        def run():
+            with torch.cuda.stream(s):
+                g.replay()
+        return run
+
+    def stage_stats(jobs, opts):
+        lib.oskar_b200_set_stage_timing(ws.handle, 1)
+        fg.grid_batch_device(ws, jobs, opts=opts, stream=s)
+        s.synchronize()
+        st = ws.stats()
+        lib.oskar_b200_set_stage_timing(ws.handle, 0)
+        return st
+
     g32 = graph_of(jobs32, plain)
-    batch32_ms = timed(g32.replay)
+    clocks = ClockSampler(local)
+    clocks.start()
+    batch32_ms = timed(replay_on_s(g32))
+    clk = clocks.stop()
     del g32
+    st = stage_stats(jobs32, plain)
+    err = {}
+    if rank == 0 and not args.no_cpu_baseline:
+        err = audit_batch(chans, cubes32, ws, plain)
     for cb in cubes32:
         cb.close()
+    del jobs32
 
     # (c) one batch, FP16 kernels + compensated accumulation, graph-captured
     cubes16, jobs16 = make_jobs(_lib.KERNEL_F16)
     comp = fg.options(accum_mode=_lib.ACCUM_COMPENSATED)
     g16 = graph_of(jobs16, comp)
-    clocks = ClockSampler(local)
-    clocks.start()
-    batch16_ms = timed(g16.replay)
-    clk = clocks.stop()
+    batch16_ms = timed(replay_on_s(g16))
     del g16
-    lib.oskar_b200_set_stage_timing(ws.handle, 1)
-    fg.grid_batch_device(ws, jobs16, opts=comp, stream=s)
-    s.synchronize()
-    st = ws.stats()
-    lib.oskar_b200_set_stage_timing(ws.handle, 0)
-
-    err = {}
+    err16 = {}
     if rank == 0 and not args.no_cpu_baseline:
-        err = audit_batch(chans, cubes16, ws)
+        err16 = audit_batch(chans, cubes16, ws, comp)
     for cb in cubes16:
         cb.close()
-    value = n_total * world / (batch16_ms * 1e-3) / 1e9
+    value = n_total * world / (batch32_ms * 1e-3) / 1e9
     return {"metric": METRIC, "value": round(value, 4), "unit": UNIT,
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": round(batch16_ms, 3), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f16 kernels, f32",
+            "ms_per_step": round(batch32_ms, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": DATA_DESC,
             "config": {"workload": BATCH_DESC, "num_points": n_total,
                        "channels": len(chans),
-                       "mode": "one graph-captured batch: FP16 kernels, "
-                               "compensated FP32 accumulation"},
+                       "mode": "one graph-captured batch: FP32 kernels and "
+                               "grids, plain accumulation",
+                       "l2": "inputs (3.9 GB/step) larger than L2; no flush"},
             "sequential_plain_fp32_ms": round(seq_ms, 3),
-            "batched_plain_fp32_ms": round(batch32_ms, 3),
-            "speedup_vs_sequential_plain_fp32": round(seq_ms / batch16_ms, 3),
-            "grid_updates_per_s": st.grid_updates * world / (batch16_ms * 1e-3),
+            "speedup_vs_sequential_plain_fp32": round(seq_ms / batch32_ms, 3),
+            "grid_updates_per_s": st.grid_updates * world / (batch32_ms * 1e-3),
             "stage_ms": {"prep": round(st.prep_ms, 3),
                          "sort": round(st.sort_ms, 3),
                          "permute_tasks": round(st.tasks_ms, 3),
-                         "grid_and_fold": round(st.grid_ms, 3)},
-            "gpu_launches_per_step": st.kernel_launches,
-            "rel_err_vs_fp64": err, "clocks": clk}
+                         "grid": round(st.grid_ms, 3)},
+            "gpu_launches": st.kernel_launches * args.steps,
+            "rel_err_vs_fp64": err,
+            "f16_compensated_batch": {
+                "ms_per_step": round(batch16_ms, 3),
+                "value": round(n_total * world / (batch16_ms * 1e-3) / 1e9, 4),
+                "rel_err_vs_fp64": err16,
+                "note": "FP16 kernel cubes quantise the kernel values to "
+                        "about 1e-4 relative, above the 1e-5 bar"},
+            "clocks": clk}
 
 
-def audit_batch(chans, cubes, ws, m=100000):
-    """Relative RMS vs the FP64 oracle of the batched FP16/compensated path on
-    seeded samples of the lowest and highest channel."""
+def audit_batch(chans, cubes, ws, opts, m=100000):
+    """Relative RMS vs the FP64 oracle of the batched path (cubes and
+    options as timed) on seeded samples of the lowest and highest
+    channel."""
     import fpga_gridding_b200 as fg
     from fpga_gridding_b200 import _lib
     O = ensure_oracle()
@@ -585,7 +610,7 @@ def audit_batch(chans, cubes, ws, m=100000):
             cube=cubes[idx], uu=sub.uu, vv=sub.vv, ww=sub.ww, vis=sub.vis,
             weight=sub.weight, cell_size_rad=hd["cell_size_rad"],
             w_scale=hd["w_scale"], grid_size=c.grid_size, grid=grid,
-            d_norm=norm)], opts=fg.options(accum_mode=_lib.ACCUM_COMPENSATED))
+            d_norm=norm)], opts=opts)
         torch.cuda.synchronize()
         out[f"channel_{idx}"] = {
             "grid_rel_rms": O.rel_rms(grid.cpu().numpy(), g_ref),
@@ -751,9 +776,222 @@ def run_serving(args, world, rank, local):
                       "fp64_oracle_jobs": len(oracle_err)}}
 
 
+WEIGHTS_DESC = ("weights: one uniform-weighting pass (weights-grid write, "
+                "then density read: oskar_grid_weights_write_f / _read_f) "
+                "over plain_large's 39,244,800 uv points with unit weights "
+                "(as main.cpp:203); 8192^2 FP32 weights grid, zero-filled "
+                "each pass; float coordinate arithmetic")
+
+
+def weights_threads(grid_size):
+    """Host threads for the weights CPU baseline: all of them, bounded by
+    memory for the private FP32 weights grids."""
+    grid_bytes = grid_size * grid_size * 4
+    t = host_threads()
+    return max(1, min(t, int(0.4 * mem_available_bytes() // grid_bytes), 256))
+
+
+def run_weights(args, world, rank, local):
+    """Uniform weighting on the GPU: ordered (bit-exact for any weights)
+    write + read per step; the atomic write is timed beside it."""
+    import fpga_gridding_b200 as fg
+    wl = make_workload(rank, args.stations)
+    n = wl.num_points
+    g = wl.grid_size
+    cell = float(np.float32(wl.cell_size_rad))
+    ws = fg.Workspace(local)
+    s = torch.cuda.Stream()
+    wgrid = torch.zeros(g * g, dtype=torch.float32, device="cuda")
+    wout = torch.zeros(n, dtype=torch.float32, device="cuda")
+    sk_w = torch.zeros(1, dtype=torch.int64, device="cuda")
+    sk_r = torch.zeros(1, dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()
+
+    def step(ordered):
+        with torch.cuda.stream(s):
+            wgrid.zero_()
+        fg.weights_write_device(ws, wl.uu, wl.vv, wl.weight, cell, g, wgrid,
+                                sk_w, ordered=ordered, stream=s)
+        fg.weights_read_device(ws, wl.uu, wl.vv, wl.weight, wout, cell, g,
+                               wgrid, sk_r, stream=s)
+
+    def timed(ordered):
+        for _ in range(args.warmup):
+            step(ordered)
+        s.synchronize()
+        barrier(world)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(args.steps):
+            step(ordered)
+        e1.record(s)
+        e1.synchronize()
+        return max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
+
+    # kernels of one pass: the write's (from the workspace statistics), the
+    # read's one kernel; the zero fill is torch's
+    fg.weights_write_device(ws, wl.uu, wl.vv, wl.weight, cell, g, wgrid,
+                            sk_w, ordered=True, stream=s)
+    s.synchronize()
+    launches_write = ws.stats().kernel_launches
+    wgrid.zero_()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ordered_ms = timed(True)
+    clk = clocks.stop()
+    g_ord = wgrid.cpu().numpy()
+    w_ord = wout.cpu().numpy()
+    skips = (int(sk_w.item()), int(sk_r.item()))
+    atomic_ms = timed(False)
+    g_atm = wgrid.cpu().numpy()
+    w_atm = wout.cpu().numpy()
+    value = n * world / (ordered_ms * 1e-3) / 1e9
+    alg_bytes = 28 * n + 16 * g * g
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (ordered_ms * 1e-3) / 1e9
+    achieved_atm = alg_bytes / (atomic_ms * 1e-3) / 1e9
+    out = {"metric": "uniform-weighting throughput (weights write + read)",
+           "value": round(value, 4), "unit": UNIT, "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": round(ordered_ms, 3), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": DATA_DESC,
+           "config": {"workload": WEIGHTS_DESC, "num_points": n,
+                      "grid_size": g, "mode": "ordered write (stable sort "
+                      "by cell, one sequential sum per cell) + read",
+                      "l2": "inputs (0.6 GB/step) larger than L2; no flush"},
+           "roofline": {"kernel": "whole pass (key, radix sort, run sum, "
+                                  "read)", "bound": "hbm",
+                        "achieved": round(achieved, 2), "peak": peak,
+                        "peak_source": peak_kind, "unit": "GB/s",
+                        "frac": round(achieved / peak, 4), "traffic": None,
+                        "algorithmic_bytes_per_launch": alg_bytes},
+           "atomic_pass": {"ms_per_step": round(atomic_ms, 3),
+                           "value": round(n * world / (atomic_ms * 1e-3)
+                                          / 1e9, 4),
+                           "hbm_frac": round(achieved_atm / peak, 4),
+                           "grid_equal_to_ordered": bool(
+                               np.array_equal(g_atm, g_ord)),
+                           "weights_equal_to_ordered": bool(
+                               np.array_equal(w_atm, w_ord))},
+           "gpu_launches": (launches_write + 1) * args.steps,
+           "skipped": {"write": skips[0], "read": skips[1]},
+           "clocks": clk}
+    if not args.no_e2e:
+        out["e2e"] = run_weights_e2e(args, wl, world)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        O = ensure_oracle()
+        use_ref = O.reference_lib() is not None
+        hd = host_dict(wl)
+        rsk_w, rg, rsk_r, rw, (tw, tr) = O.weights_timed(
+            hd["uu"], hd["vv"], hd["weight"], hd["cell_size_rad"], g,
+            np.zeros(g * g, np.float32), np.zeros(n, np.float32),
+            single=True, use_reference=use_ref)
+        kind = "reference" if use_ref else "port"
+        t = weights_threads(g)
+        secs, _, _, _, _ = O.time_weights_parallel(
+            hd["uu"], hd["vv"], hd["weight"], hd["cell_size_rad"], g, t,
+            use_ref)
+        out["cpu_baseline"] = {
+            "value": round(n / secs / 1e9, 6), "unit": UNIT, "cores": t,
+            "kind": kind,
+            "serial_value": round(n / (tw + tr) / 1e9, 6),
+            "sample": f"the whole workload, once: {'reference' if use_ref else 'restated'} "
+                      f"oskar_grid_weights_write_f on {t} threads with "
+                      f"private grids over slices, a parallel sum of the "
+                      f"grids, then _read_f over slices; {secs:.3f} s "
+                      f"(serial_value: one thread, {tw + tr:.3f} s)"}
+        out["parity_vs_reference"] = {
+            "skipped_equal": (rsk_w, rsk_r) == skips,
+            "grid_bit_exact": bool(np.array_equal(rg, g_ord)),
+            "weights_bit_exact": bool(np.array_equal(rw, w_ord)),
+            "atomic_grid_bit_exact": bool(np.array_equal(rg, g_atm)),
+            "sample": "the whole workload"}
+    return out
+
+
+def run_weights_e2e(args, wl, world):
+    """oskar_grid_weights_write_f then _read_f (drop-in C ABI) on pinned
+    host buffers, K steps."""
+    import fpga_gridding_b200 as fg
+    pin = lambda t: t.cpu().pin_memory()
+    h = {k: pin(getattr(wl, k)).numpy() for k in ("uu", "vv", "weight")}
+    n = wl.num_points
+    g = wl.grid_size
+    hgrid = torch.zeros(g * g, dtype=torch.float32).pin_memory().numpy()
+    hout = torch.zeros(n, dtype=torch.float32).pin_memory().numpy()
+    cell = float(np.float32(wl.cell_size_rad))
+
+    def call():
+        hgrid[:] = 0.0
+        fg.oskar_grid_weights_write_f(n, h["uu"], h["vv"], h["weight"], cell,
+                                      g, hgrid)
+        fg.oskar_grid_weights_read_f(n, h["uu"], h["vv"], h["weight"], hout,
+                                     cell, g, hgrid)
+    for _ in range(max(1, args.warmup)):
+        call()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        call()
+    secs = max_over_ranks(time.perf_counter() - t0, world)
+    fg.load().oskar_grid_wproj_b200_release_thread_cache()
+    return {"value": round(n * args.steps * world / secs / 1e9, 4),
+            "unit": UNIT,
+            "h2d_bytes_per_step": n * 12 + n * 16 + 2 * g * g * 4,
+            "d2h_bytes_per_step": g * g * 4 + n * 4 + 16,
+            "ms_per_step": round(1e3 * secs / args.steps, 3),
+            "path": "oskar_grid_weights_write_f + _read_f (drop-in C ABI), "
+                    "pinned host buffers; the host zero fill of the weights "
+                    "grid is inside the timed region"}
+
+
+def run_reference_weights(args, world):
+    """Reference arm of the weights workload: the reference's serial
+    oskar_grid_weights_write_f + _read_f over the whole workload per step."""
+    O = ensure_oracle()
+    use_ref = O.reference_lib() is not None
+    wl = make_workload(0)
+    hd = host_dict(wl)
+    n = len(hd["uu"])
+    g = hd["grid_size"]
+    del wl
+    t = weights_threads(g)
+    tot = 0.0
+    for i in range(args.warmup + args.steps):
+        secs, _, _, _, _ = O.time_weights_parallel(
+            hd["uu"], hd["vv"], hd["weight"], hd["cell_size_rad"], g, t,
+            use_ref)
+        if i >= args.warmup:
+            tot += secs
+    value = n * args.steps / tot / 1e9
+    kind = "reference" if use_ref else "port"
+    return {"impl": "reference",
+            "metric": "uniform-weighting throughput (weights write + read)",
+            "value": round(value, 6), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(1e3 * tot / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": DATA_DESC,
+            "config": {"workload": WEIGHTS_DESC, "num_points": n,
+                       "grid_size": g},
+            "cpu_baseline": {"value": round(value, 6), "unit": UNIT,
+                             "cores": t, "kind": kind,
+                             "sample": f"each step: the whole workload; "
+                                       f"oskar_grid_weights_write_f on {t} "
+                                       f"threads with private grids over "
+                                       f"slices, a parallel sum of the "
+                                       f"grids, then _read_f over slices"},
+            "e2e": {"value": round(value, 6), "unit": UNIT,
+                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return None
+    if args.workload == "weights":
+        return run_reference_weights(args, world)
     O = ensure_oracle()
     use_ref = O.reference_lib() is not None
     wl = make_workload(0)
@@ -804,11 +1042,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", choices=("plain_large", "batch128",
-                                           "serving"),
+                                           "serving", "weights"),
                     default="plain_large",
                     help="plain_large (the benchmark job), batch128 (the "
-                         "128-channel batching workload) or serving (the "
-                         "Poisson job stream)")
+                         "128-channel batching workload), serving (the "
+                         "Poisson job stream) or weights (uniform "
+                         "weighting over the benchmark job's uv points)")
     ap.add_argument("--serving-jobs", type=int, default=2000)
     ap.add_argument("--stations", type=int, default=512,
                     help="stations of the job (512 = the benchmark job; "
@@ -829,6 +1068,8 @@ def main():
             out = run_batch128(args, world, rank, local)
         elif args.workload == "serving":
             out = run_serving(args, world, rank, local)
+        elif args.workload == "weights":
+            out = run_weights(args, world, rank, local)
         else:
             out = run_b200(args, world, rank, local)
         if rank == 0 and out is not None:

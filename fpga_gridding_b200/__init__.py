@@ -9,5 +9,8 @@ calling any gridding function does, and fails loudly if it is missing.
 from ._lib import EXPORTED_SYMBOLS, GridderError, LIB_PATH, load  # noqa: F401
 from .gridder import (Cube, Workspace, grid_batch_device, grid_device,  # noqa: F401
                       grid_workload,
-                      options, oskar_grid_wproj_d, oskar_grid_wproj_f,
-                      place_device)
+                      options, oskar_grid_weights_read_d,
+                      oskar_grid_weights_read_f, oskar_grid_weights_write_d,
+                      oskar_grid_weights_write_f, oskar_grid_wproj_d,
+                      oskar_grid_wproj_f, place_device, weights_read_device,
+                      weights_write_device)

@@ -13,6 +13,10 @@ LIB_PATH = os.path.join(HERE, "libgridder_b200.so")
 EXPORTED_SYMBOLS = (
     "oskar_grid_wproj_d",
     "oskar_grid_wproj_f",
+    "oskar_grid_weights_write_d",
+    "oskar_grid_weights_read_d",
+    "oskar_grid_weights_write_f",
+    "oskar_grid_weights_read_f",
     "oskar_grid_wproj_b200_last_error",
     "oskar_grid_wproj_b200_error_string",
     "oskar_grid_wproj_b200_release_thread_cache",
@@ -26,6 +30,8 @@ EXPORTED_SYMBOLS = (
     "oskar_b200_grid",
     "oskar_b200_grid_batch",
     "oskar_b200_place",
+    "oskar_b200_weights_write",
+    "oskar_b200_weights_read",
     "oskar_b200_last_stats",
     "oskar_b200_set_stage_timing",
     "oskar_b200_measure_atomic_rate",
@@ -37,6 +43,7 @@ EXPORTED_SYMBOLS = (
     "oskar_b200_server_clock",
     "oskar_b200_server_memory",
     "oskar_b200_server_free",
+    "oskar_b200_selftest_bounded_wait",
     "oskar_b200_build_info",
 )
 
@@ -123,6 +130,18 @@ def load():
     lib.oskar_grid_wproj_f.argtypes = grid_common + [
         C.c_float, C.c_float, C.c_int, _P, _P, _P]
     lib.oskar_grid_wproj_d.restype = lib.oskar_grid_wproj_f.restype = None
+    for t, real in (("d", C.c_double), ("f", C.c_float)):
+        fw = getattr(lib, "oskar_grid_weights_write_" + t)
+        fw.argtypes = [_SZ, _P, _P, _P, real, C.c_int, _P, _P]
+        fw.restype = None
+        fr = getattr(lib, "oskar_grid_weights_read_" + t)
+        fr.argtypes = [_SZ, _P, _P, _P, _P, real, C.c_int, _P, _P]
+        fr.restype = None
+    lib.oskar_b200_weights_write.argtypes = [
+        _P, C.c_int, C.c_int, _SZ, _P, _P, _P, C.c_double, C.c_int, _P, _P,
+        _P]
+    lib.oskar_b200_weights_read.argtypes = [
+        _P, C.c_int, _SZ, _P, _P, _P, _P, C.c_double, C.c_int, _P, _P, _P]
     lib.oskar_grid_wproj_b200_last_error.restype = C.c_int
     lib.oskar_grid_wproj_b200_error_string.argtypes = [C.c_int]
     lib.oskar_grid_wproj_b200_error_string.restype = C.c_char_p
@@ -156,6 +175,9 @@ def load():
         _SZ, _P, C.c_int, C.c_int, _P, _SZ, _P, _P, _P, _P, C.c_float,
         C.c_float, C.c_int, _P, _P, _P, _P]
     lib.oskar_b200_grid_f_static.restype = C.c_int
+    lib.oskar_b200_selftest_bounded_wait.argtypes = [_P, C.c_uint,
+                                                     C.POINTER(C.c_int)]
+    lib.oskar_b200_selftest_bounded_wait.restype = C.c_int
     lib.oskar_b200_server_create.argtypes = [C.c_int, _SZ, C.c_int, C.c_int,
                                              C.POINTER(Options),
                                              C.POINTER(_P)]

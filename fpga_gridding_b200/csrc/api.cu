@@ -651,3 +651,249 @@ const char* oskar_b200_build_info(void)
 }
 
 }  // extern "C"
+
+extern "C" int oskar_b200_selftest_bounded_wait(oskar_B200Workspace* ws,
+                                                unsigned spins,
+                                                int* device_status)
+{
+    if (!ws || !device_status || spins == 0)
+        return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    DeviceGuard g(ws->device);
+    return selftest_bounded_wait(ws, spins, device_status);
+}
+
+// ---------------------------------------------------------------------------
+// Uniform weighting: drop-ins for utils/oskar_grid_weights.c and the
+// device-resident calls.
+// ---------------------------------------------------------------------------
+namespace {
+
+int check_weights_args(size_t num_points, const void* uu, const void* vv,
+                       const void* weight, int grid_size, const void* grid)
+{
+    if (grid_size < 1 || grid_size > 65535 || !grid)
+        return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    if (num_points >= 0xffffffffull) return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    if (num_points && (!uu || !vv || !weight))
+        return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    return OSKAR_B200_OK;
+}
+
+// The calling thread's cached workspace on its current device.
+int dropin_workspace(oskar_B200Workspace** out)
+{
+    int device = 0;
+    int st = current_device(&device);
+    if (st) return st;
+    ThreadCache& tc = tls_cache;
+    if (tc.ws && tc.ws->device != device) tc.release();
+    if (!tc.ws)
+    {
+        st = workspace_create(device, &tc.ws);
+        if (st) return st;
+    }
+    *out = tc.ws;
+    return OSKAR_B200_OK;
+}
+
+#define B200_WCHECK(expr)                                           \
+    do {                                                            \
+        const cudaError_t e_ = (expr);                              \
+        if (e_ != cudaSuccess) { cudaStreamSynchronize(s);          \
+                                 cudaGetLastError();                \
+                                 return status_from_cuda(e_); }     \
+    } while (0)
+
+// oskar_grid_weights_write_{d,f} on host arrays: ordered (bit-exact) write.
+template <typename T>
+int weights_write_drop_in(size_t n, const T* uu, const T* vv,
+                          const T* weight, double cell_size_rad,
+                          int grid_size, size_t* num_skipped, T* grid)
+{
+    if (!num_skipped) return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    int st = check_weights_args(n, uu, vv, weight, grid_size, grid);
+    if (st) return st;
+    oskar_B200Workspace* ws = nullptr;
+    st = dropin_workspace(&ws);
+    if (st) return st;
+    cudaStream_t s = ws->stream;
+    const size_t grid_bytes = (size_t)grid_size * grid_size * sizeof(T);
+    B200_WCHECK(ws->in_grid.ensure(grid_bytes));
+    B200_WCHECK(ws->in_norm.ensure(2 * sizeof(double)));
+    if (n)
+    {
+        B200_WCHECK(ws->in_uu.ensure(n * sizeof(T)));
+        B200_WCHECK(ws->in_vv.ensure(n * sizeof(T)));
+        B200_WCHECK(ws->in_weight.ensure(n * sizeof(T)));
+        B200_WCHECK(cudaMemcpyAsync(ws->in_uu.ptr, uu, n * sizeof(T),
+                                    cudaMemcpyHostToDevice, s));
+        B200_WCHECK(cudaMemcpyAsync(ws->in_vv.ptr, vv, n * sizeof(T),
+                                    cudaMemcpyHostToDevice, s));
+        B200_WCHECK(cudaMemcpyAsync(ws->in_weight.ptr, weight, n * sizeof(T),
+                                    cudaMemcpyHostToDevice, s));
+    }
+    B200_WCHECK(cudaMemcpyAsync(ws->in_grid.ptr, grid, grid_bytes,
+                                cudaMemcpyHostToDevice, s));
+    unsigned long long* d_skip =
+        static_cast<unsigned long long*>(ws->in_norm.ptr);
+    st = run_weights_write(ws, sizeof(T) == sizeof(double), 1, n,
+                           ws->in_uu.ptr, ws->in_vv.ptr, ws->in_weight.ptr,
+                           cell_size_rad, grid_size, ws->in_grid.ptr, d_skip,
+                           s);
+    if (st) { cudaStreamSynchronize(s); cudaGetLastError(); return st; }
+    B200_WCHECK(cudaStreamSynchronize(s));
+    unsigned long long skipped = 0;
+    B200_WCHECK(cudaMemcpyAsync(&skipped, d_skip, sizeof(skipped),
+                                cudaMemcpyDeviceToHost, s));
+    B200_WCHECK(cudaMemcpyAsync(grid, ws->in_grid.ptr, grid_bytes,
+                                cudaMemcpyDeviceToHost, s));
+    B200_WCHECK(cudaStreamSynchronize(s));
+    *num_skipped = (size_t)skipped;
+    return OSKAR_B200_OK;
+}
+
+// oskar_grid_weights_read_{d,f} on host arrays.  weight_out is uploaded as
+// well: the entries of skipped points keep their previous values.
+template <typename T>
+int weights_read_drop_in(size_t n, const T* uu, const T* vv,
+                         const T* weight_in, T* weight_out,
+                         double cell_size_rad, int grid_size,
+                         size_t* num_skipped, const T* grid)
+{
+    if (!num_skipped || (n && !weight_out))
+        return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    int st = check_weights_args(n, uu, vv, weight_in, grid_size, grid);
+    if (st) return st;
+    oskar_B200Workspace* ws = nullptr;
+    st = dropin_workspace(&ws);
+    if (st) return st;
+    cudaStream_t s = ws->stream;
+    const size_t grid_bytes = (size_t)grid_size * grid_size * sizeof(T);
+    B200_WCHECK(ws->in_grid.ensure(grid_bytes));
+    B200_WCHECK(ws->in_norm.ensure(2 * sizeof(double)));
+    if (n)
+    {
+        B200_WCHECK(ws->in_uu.ensure(n * sizeof(T)));
+        B200_WCHECK(ws->in_vv.ensure(n * sizeof(T)));
+        B200_WCHECK(ws->in_weight.ensure(n * sizeof(T)));
+        B200_WCHECK(ws->in_vis.ensure(n * sizeof(T)));
+        B200_WCHECK(cudaMemcpyAsync(ws->in_uu.ptr, uu, n * sizeof(T),
+                                    cudaMemcpyHostToDevice, s));
+        B200_WCHECK(cudaMemcpyAsync(ws->in_vv.ptr, vv, n * sizeof(T),
+                                    cudaMemcpyHostToDevice, s));
+        B200_WCHECK(cudaMemcpyAsync(ws->in_weight.ptr, weight_in,
+                                    n * sizeof(T), cudaMemcpyHostToDevice,
+                                    s));
+        B200_WCHECK(cudaMemcpyAsync(ws->in_vis.ptr, weight_out,
+                                    n * sizeof(T), cudaMemcpyHostToDevice,
+                                    s));
+    }
+    B200_WCHECK(cudaMemcpyAsync(ws->in_grid.ptr, grid, grid_bytes,
+                                cudaMemcpyHostToDevice, s));
+    unsigned long long* d_skip =
+        static_cast<unsigned long long*>(ws->in_norm.ptr);
+    st = run_weights_read(ws, sizeof(T) == sizeof(double), n, ws->in_uu.ptr,
+                          ws->in_vv.ptr, ws->in_weight.ptr, ws->in_vis.ptr,
+                          cell_size_rad, grid_size, ws->in_grid.ptr, d_skip,
+                          s);
+    if (st) { cudaStreamSynchronize(s); cudaGetLastError(); return st; }
+    B200_WCHECK(cudaStreamSynchronize(s));
+    unsigned long long skipped = 0;
+    B200_WCHECK(cudaMemcpyAsync(&skipped, d_skip, sizeof(skipped),
+                                cudaMemcpyDeviceToHost, s));
+    if (n)
+        B200_WCHECK(cudaMemcpyAsync(weight_out, ws->in_vis.ptr,
+                                    n * sizeof(T), cudaMemcpyDeviceToHost,
+                                    s));
+    B200_WCHECK(cudaStreamSynchronize(s));
+    *num_skipped = (size_t)skipped;
+    return OSKAR_B200_OK;
+}
+
+#undef B200_WCHECK
+
+}  // namespace
+
+extern "C" {
+
+void oskar_grid_weights_write_d(const size_t num_points, const double* uu,
+                                const double* vv, const double* weight,
+                                const double cell_size_rad,
+                                const int grid_size, size_t* num_skipped,
+                                double* grid)
+{
+    tls_status = weights_write_drop_in<double>(num_points, uu, vv, weight,
+                                               cell_size_rad, grid_size,
+                                               num_skipped, grid);
+}
+
+void oskar_grid_weights_read_d(const size_t num_points, const double* uu,
+                               const double* vv, const double* weight_in,
+                               double* weight_out, const double cell_size_rad,
+                               const int grid_size, size_t* num_skipped,
+                               const double* grid)
+{
+    tls_status = weights_read_drop_in<double>(num_points, uu, vv, weight_in,
+                                              weight_out, cell_size_rad,
+                                              grid_size, num_skipped, grid);
+}
+
+void oskar_grid_weights_write_f(const size_t num_points, const float* uu,
+                                const float* vv, const float* weight,
+                                const float cell_size_rad,
+                                const int grid_size, size_t* num_skipped,
+                                float* grid)
+{
+    tls_status = weights_write_drop_in<float>(num_points, uu, vv, weight,
+                                              (double)cell_size_rad,
+                                              grid_size, num_skipped, grid);
+}
+
+void oskar_grid_weights_read_f(const size_t num_points, const float* uu,
+                               const float* vv, const float* weight_in,
+                               float* weight_out, const float cell_size_rad,
+                               const int grid_size, size_t* num_skipped,
+                               const float* grid)
+{
+    tls_status = weights_read_drop_in<float>(num_points, uu, vv, weight_in,
+                                             weight_out,
+                                             (double)cell_size_rad,
+                                             grid_size, num_skipped, grid);
+}
+
+int oskar_b200_weights_write(oskar_B200Workspace* ws, int data_is_double,
+                             int ordered, size_t num_points, const void* uu,
+                             const void* vv, const void* weight,
+                             double cell_size_rad, int grid_size, void* grid,
+                             unsigned long long* d_num_skipped, void* stream)
+{
+    if (!ws) return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    int st = check_weights_args(num_points, uu, vv, weight, grid_size, grid);
+    if (st) return st;
+    DeviceGuard g(ws->device);
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ws->stream;
+    return run_weights_write(ws, data_is_double ? 1 : 0, ordered ? 1 : 0,
+                             num_points, uu, vv, weight, cell_size_rad,
+                             grid_size, grid, d_num_skipped, s);
+}
+
+int oskar_b200_weights_read(oskar_B200Workspace* ws, int data_is_double,
+                            size_t num_points, const void* uu,
+                            const void* vv, const void* weight_in,
+                            void* weight_out, double cell_size_rad,
+                            int grid_size, const void* grid,
+                            unsigned long long* d_num_skipped, void* stream)
+{
+    if (!ws || (num_points && !weight_out))
+        return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    int st = check_weights_args(num_points, uu, vv, weight_in, grid_size,
+                                grid);
+    if (st) return st;
+    DeviceGuard g(ws->device);
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ws->stream;
+    return run_weights_read(ws, data_is_double ? 1 : 0, num_points, uu, vv,
+                            weight_in, weight_out, cell_size_rad, grid_size,
+                            grid, d_num_skipped, s);
+}
+
+}  // extern "C"

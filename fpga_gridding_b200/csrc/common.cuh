@@ -79,9 +79,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
 
 // Bounded wait; returns false when the iteration limit ran out.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar,
-                                                  uint32_t parity)
+                                                  uint32_t parity,
+                                                  unsigned limit = kSpinLimit)
 {
-    for (unsigned i = 0; i < kSpinLimit; ++i)
+    for (unsigned i = 0; i < limit; ++i)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }

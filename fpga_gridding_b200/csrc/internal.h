@@ -235,6 +235,23 @@ int run_place(oskar_B200Workspace* ws, int data_is_double, int coord_mode,
 int measure_atomic_rate(oskar_B200Workspace* ws, void* grid, int grid_size,
                         int iters, double* updates_per_s);
 
+// ---- weights.cu -------------------------------------------------------------
+// Uniform weighting (utils/oskar_grid_weights.c:38-172) on device arrays.
+// *d_num_skipped (or a workspace counter when null) is reset, then counts.
+int run_weights_write(oskar_B200Workspace* ws, int data_is_double,
+                      int ordered, size_t n, const void* uu, const void* vv,
+                      const void* weight, double cell_size_rad,
+                      int grid_size, void* grid,
+                      unsigned long long* d_num_skipped, cudaStream_t st);
+int run_weights_read(oskar_B200Workspace* ws, int data_is_double, size_t n,
+                     const void* uu, const void* vv, const void* weight_in,
+                     void* weight_out, double cell_size_rad, int grid_size,
+                     const void* grid, unsigned long long* d_num_skipped,
+                     cudaStream_t st);
+
+int selftest_bounded_wait(oskar_B200Workspace* ws, unsigned spins,
+                          int* device_status);
+
 int status_from_cuda(cudaError_t e);
 
 }  // namespace b200

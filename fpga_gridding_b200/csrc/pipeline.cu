@@ -375,7 +375,45 @@ __global__ void atomic_rate_kernel(float* __restrict__ grid, int grid_size,
     }
 }
 
+// Self-test of the bounded waits: one CTA waits on an mbarrier phase that
+// nothing completes (no arrival is ever made), gives up after `spins`
+// try_wait attempts and records DEV_ERR_TIMEOUT, exactly as the gridding
+// kernel does when a staged copy never lands.
+__global__ void bounded_wait_probe_kernel(unsigned spins,
+                                          unsigned long long* status)
+{
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0)
+    {
+        mbar_init(&bar, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    const bool ok = mbar_wait_bounded(&bar, 0, spins);
+    if (!__syncthreads_and(ok) && threadIdx.x == 0)
+        atomicOr(status, (unsigned long long)DEV_ERR_TIMEOUT);
+}
+
 }  // namespace
+
+int selftest_bounded_wait(oskar_B200Workspace* ws, unsigned spins,
+                          int* device_status)
+{
+    B200_TRY(ws->counters.ensure(sizeof(unsigned long long) * CNT_COUNT));
+    unsigned long long* c = static_cast<unsigned long long*>(ws->counters.ptr);
+    B200_TRY(cudaMemsetAsync(c, 0, sizeof(unsigned long long) * CNT_COUNT,
+                             ws->stream));
+    bounded_wait_probe_kernel<<<1, 128, 0, ws->stream>>>(spins,
+                                                         c + CNT_STATUS);
+    B200_TRY(cudaGetLastError());
+    unsigned long long s = 0;
+    B200_TRY(cudaMemcpyAsync(&s, c + CNT_STATUS, sizeof(s),
+                             cudaMemcpyDeviceToHost, ws->stream));
+    B200_TRY(cudaStreamSynchronize(ws->stream));
+    *device_status = (s & DEV_ERR_TIMEOUT) ? OSKAR_B200_ERR_TIMEOUT
+                                           : OSKAR_B200_OK;
+    return OSKAR_B200_OK;
+}
 
 int measure_atomic_rate(oskar_B200Workspace* ws, void* grid, int grid_size,
                         int iters, double* updates_per_s)

@@ -83,6 +83,59 @@ def grid_workload(w: dict, single: bool, grid=None, norm: float = 0.0):
     return sk, nrm, grid
 
 
+def _weights_write(t, real, num_points, uu, vv, weight, cell_size_rad,
+                   grid_size, grid):
+    lib = load()
+    fn = getattr(lib, "oskar_grid_weights_write_" + t)
+    skipped = C.c_size_t(0)
+    fn(num_points, _carr(uu, real), _carr(vv, real), _carr(weight, real),
+       cell_size_rad, grid_size, C.byref(skipped), _carr(grid, real))
+    check(lib.oskar_grid_wproj_b200_last_error(), fn.__name__)
+    return skipped.value
+
+
+def _weights_read(t, real, num_points, uu, vv, weight_in, weight_out,
+                  cell_size_rad, grid_size, grid):
+    lib = load()
+    fn = getattr(lib, "oskar_grid_weights_read_" + t)
+    skipped = C.c_size_t(0)
+    fn(num_points, _carr(uu, real), _carr(vv, real), _carr(weight_in, real),
+       _carr(weight_out, real), cell_size_rad, grid_size, C.byref(skipped),
+       _carr(grid, real))
+    check(lib.oskar_grid_wproj_b200_last_error(), fn.__name__)
+    return skipped.value
+
+
+def oskar_grid_weights_write_d(num_points, uu, vv, weight, cell_size_rad,
+                               grid_size, grid):
+    """utils/oskar_grid_weights.c:38-69 on the GPU.  grid (grid_size^2
+    float64) accumulates in place; returns num_skipped."""
+    return _weights_write("d", np.float64, num_points, uu, vv, weight,
+                          cell_size_rad, grid_size, grid)
+
+
+def oskar_grid_weights_read_d(num_points, uu, vv, weight_in, weight_out,
+                              cell_size_rad, grid_size, grid):
+    """utils/oskar_grid_weights.c:71-103 on the GPU.  weight_out is updated
+    in place; returns num_skipped."""
+    return _weights_read("d", np.float64, num_points, uu, vv, weight_in,
+                         weight_out, cell_size_rad, grid_size, grid)
+
+
+def oskar_grid_weights_write_f(num_points, uu, vv, weight, cell_size_rad,
+                               grid_size, grid):
+    """utils/oskar_grid_weights.c:105-136 (float) on the GPU."""
+    return _weights_write("f", np.float32, num_points, uu, vv, weight,
+                          cell_size_rad, grid_size, grid)
+
+
+def oskar_grid_weights_read_f(num_points, uu, vv, weight_in, weight_out,
+                              cell_size_rad, grid_size, grid):
+    """utils/oskar_grid_weights.c:138-170 (float) on the GPU."""
+    return _weights_read("f", np.float32, num_points, uu, vv, weight_in,
+                         weight_out, cell_size_rad, grid_size, grid)
+
+
 # --------------------------------------------------------------------------
 # Extended API (device-resident, torch tensors)
 # --------------------------------------------------------------------------
@@ -253,3 +306,28 @@ def place_device(ws: Workspace, support, oversample: int, uu, vv, ww,
                                  "conj", "skipped")],
         _stream_ptr(stream)), "oskar_b200_place")
     return out
+
+
+def weights_write_device(ws: Workspace, uu, vv, weight, cell_size_rad,
+                         grid_size: int, grid, num_skipped=None,
+                         ordered: bool = True, stream=None):
+    """Weights-grid histogram on torch CUDA tensors (float32 or float64);
+    grid (grid_size^2 reals) accumulates.  ordered=True is bit-identical to
+    the reference; ordered=False uses one atomic add per point."""
+    dbl = uu.dtype.is_floating_point and uu.element_size() == 8
+    check(ws._lib.oskar_b200_weights_write(
+        ws.handle, int(dbl), int(ordered), uu.numel(), _ptr(uu), _ptr(vv),
+        _ptr(weight), float(cell_size_rad), grid_size, _ptr(grid),
+        _ptr(num_skipped), _stream_ptr(stream)), "weights_write")
+
+
+def weights_read_device(ws: Workspace, uu, vv, weight_in, weight_out,
+                        cell_size_rad, grid_size: int, grid,
+                        num_skipped=None, stream=None):
+    """Density lookup on torch CUDA tensors: weight_out = weight_in /
+    grid[cell] (0 for empty cells; skipped points keep weight_out)."""
+    dbl = uu.element_size() == 8
+    check(ws._lib.oskar_b200_weights_read(
+        ws.handle, int(dbl), uu.numel(), _ptr(uu), _ptr(vv), _ptr(weight_in),
+        _ptr(weight_out), float(cell_size_rad), grid_size, _ptr(grid),
+        _ptr(num_skipped), _stream_ptr(stream)), "weights_read")

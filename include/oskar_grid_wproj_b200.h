@@ -103,6 +103,39 @@ void oskar_grid_wproj_f(
         double* norm,
         float* grid);
 
+/* Replace oskar_grid_weights_{write,read}_{d,f} (utils/oskar_grid_weights.h:
+ * 60-65, 84-89, 107-112, 131-136): the "uniform" weighting histogram and its
+ * density lookup, computed on the GPU on the caller's host arrays.  Same
+ * arguments and results as the reference, bit for bit:
+ *   write: grid (real, grid_size^2, row-major in v) += weight of every point
+ *     at cell (round(-u * grid_size * cell) + grid_size / 2,
+ *     round(v * grid_size * cell) + grid_size / 2); each cell's weights are
+ *     added in point order (a stable sort by cell on the device, then one
+ *     sequential sum per cell); num_skipped counts points outside the grid.
+ *   read: weight_out[i] = weight_in[i] / grid[cell], or 0 where the cell
+ *     is empty; skipped points keep their weight_out value.
+ * The _f variants do the coordinate arithmetic in float, as the reference's.
+ * Synchronous; on failure the outputs are untouched and the status is
+ * available from oskar_grid_wproj_b200_last_error(). */
+OSKAR_B200_EXPORT
+void oskar_grid_weights_write_d(const size_t num_points, const double* uu,
+        const double* vv, const double* weight, const double cell_size_rad,
+        const int grid_size, size_t* num_skipped, double* grid);
+OSKAR_B200_EXPORT
+void oskar_grid_weights_read_d(const size_t num_points, const double* uu,
+        const double* vv, const double* weight_in, double* weight_out,
+        const double cell_size_rad, const int grid_size, size_t* num_skipped,
+        const double* grid);
+OSKAR_B200_EXPORT
+void oskar_grid_weights_write_f(const size_t num_points, const float* uu,
+        const float* vv, const float* weight, const float cell_size_rad,
+        const int grid_size, size_t* num_skipped, float* grid);
+OSKAR_B200_EXPORT
+void oskar_grid_weights_read_f(const size_t num_points, const float* uu,
+        const float* vv, const float* weight_in, float* weight_out,
+        const float cell_size_rad, const int grid_size, size_t* num_skipped,
+        const float* grid);
+
 /* Status of the calling thread's most recent drop-in call. */
 OSKAR_B200_EXPORT int oskar_grid_wproj_b200_last_error(void);
 
@@ -244,6 +277,29 @@ OSKAR_B200_EXPORT int oskar_b200_place(oskar_B200Workspace* ws,
         int32_t* gu, int32_t* gv, int32_t* plane, int32_t* off_u,
         int32_t* off_v, int32_t* conj, int32_t* skipped, void* stream);
 
+/* Uniform weighting on device arrays (FP64 when data_is_double, else FP32
+ * with the reference's float coordinate arithmetic), asynchronous on
+ * `stream`.  *d_num_skipped (device, may be NULL) is reset, then counts the
+ * points outside the grid.
+ * write: grid (device, grid_size^2 reals) accumulates the weights.
+ *   ordered = 1 adds each cell's weights in point order, bit-identical to
+ *   oskar_grid_weights_write_{d,f} (stable sort by cell, then one
+ *   sequential sum per cell); ordered = 0 issues one atomic add per point
+ *   (faster; cell sums depend on the order the atomics land in, exact when
+ *   every partial sum is, e.g. unit weights).
+ * read: weight_out[i] = weight_in[i] / grid[cell] (0 for an empty cell);
+ *   skipped points keep their weight_out value. */
+OSKAR_B200_EXPORT int oskar_b200_weights_write(oskar_B200Workspace* ws,
+        int data_is_double, int ordered, size_t num_points, const void* uu,
+        const void* vv, const void* weight, double cell_size_rad,
+        int grid_size, void* grid, unsigned long long* d_num_skipped,
+        void* stream);
+OSKAR_B200_EXPORT int oskar_b200_weights_read(oskar_B200Workspace* ws,
+        int data_is_double, size_t num_points, const void* uu, const void* vv,
+        const void* weight_in, void* weight_out, double cell_size_rad,
+        int grid_size, const void* grid, unsigned long long* d_num_skipped,
+        void* stream);
+
 /* Statistics of the most recent oskar_b200_grid call on this workspace
  * (valid once its stream has been synchronised). */
 typedef struct oskar_B200Stats
@@ -367,6 +423,14 @@ OSKAR_B200_EXPORT int oskar_b200_server_memory(oskar_B200Server* server,
         size_t* bytes_in_use, size_t* budget);
 /* Drains all jobs, frees every grid and workspace, stops the thread. */
 OSKAR_B200_EXPORT int oskar_b200_server_free(oskar_B200Server* server);
+
+/* Self-test of the device-side bounded waits: a kernel waits on a barrier
+ * phase that nothing completes, gives up after `spins` attempts and records
+ * a timeout in the workspace's status word, leaving the context usable.
+ * *device_status receives OSKAR_B200_ERR_TIMEOUT when the wait expired as
+ * designed.  Synchronous. */
+OSKAR_B200_EXPORT int oskar_b200_selftest_bounded_wait(
+        oskar_B200Workspace* ws, unsigned spins, int* device_status);
 
 /* Library build description (arch, version). */
 OSKAR_B200_EXPORT const char* oskar_b200_build_info(void);

@@ -826,3 +826,127 @@ double orc_time_parallel_f(orc_grid_fn_f fn, int num_threads,
             num_points, uu, vv, ww, vis, weight, (double)cell_size_rad,
             (double)w_scale, grid_size, skipped_out, norm_out, grid_out);
 }
+
+/* ------------------------------------------------------------------ */
+/* CPU baseline harness for uniform weighting (FP32): the weights write */
+/* on private grids over contiguous slices, a parallel sum of the       */
+/* private grids, then the read over slices of the summed grid.         */
+/* ------------------------------------------------------------------ */
+
+typedef struct
+{
+    orc_wwrite_fn_f wfn;
+    orc_wread_fn_f rfn;
+    int t, num_threads;
+    size_t begin, end, num_points, cells;
+    const float *uu, *vv, *w_in;
+    float* w_out;
+    float cell_size_rad;
+    int grid_size;
+    float* grid;            /* private grid */
+    float** grids;          /* every thread's private grid */
+    float* grid_out;        /* summed grid */
+    size_t skipped_w, skipped_r;
+    int failed;
+    double seconds;
+    pthread_barrier_t* barrier;
+} WeightsJob;
+
+static void* weights_worker(void* arg)
+{
+    WeightsJob* job = (WeightsJob*)arg;
+    const size_t n = job->end - job->begin;
+    size_t c, c0, c1, sk = 0;
+    double t0;
+    int k;
+    job->grid = (float*)malloc(job->cells * sizeof(float));
+    if (job->grid) memset(job->grid, 0, job->cells * sizeof(float));
+    else job->failed = 1;
+    job->grids[job->t] = job->grid;
+    pthread_barrier_wait(job->barrier);
+    t0 = now_s();
+    if (job->grid)
+    {
+        job->wfn(n, job->uu + job->begin, job->vv + job->begin,
+                 job->w_in + job->begin, job->cell_size_rad, job->grid_size,
+                 &sk, job->grid);
+        job->skipped_w = sk;
+    }
+    pthread_barrier_wait(job->barrier);
+    /* this thread's share of the cells, summed over all private grids in
+     * thread order */
+    c0 = (job->cells * (size_t)job->t) / (size_t)job->num_threads;
+    c1 = (job->cells * (size_t)(job->t + 1)) / (size_t)job->num_threads;
+    for (k = 0; k < job->num_threads; ++k)
+    {
+        const float* src = job->grids[k];
+        if (!src) continue;
+        for (c = c0; c < c1; ++c) job->grid_out[c] += src[c];
+    }
+    pthread_barrier_wait(job->barrier);
+    job->rfn(n, job->uu + job->begin, job->vv + job->begin,
+             job->w_in + job->begin, job->w_out + job->begin,
+             job->cell_size_rad, job->grid_size, &sk, job->grid_out);
+    job->skipped_r = sk;
+    job->seconds = now_s() - t0;
+    return NULL;
+}
+
+double orc_time_weights_parallel_f(orc_wwrite_fn_f wfn, orc_wread_fn_f rfn,
+        int num_threads, size_t num_points, const float* uu, const float* vv,
+        const float* w_in, float cell_size_rad, int grid_size,
+        float* grid_out, float* w_out, size_t* skipped_w, size_t* skipped_r)
+{
+    const size_t cells = (size_t)grid_size * (size_t)grid_size;
+    WeightsJob* jobs;
+    pthread_t* th;
+    float** grids;
+    pthread_barrier_t barrier;
+    double worst = 0.0;
+    int t;
+    if (num_threads < 1) num_threads = 1;
+    jobs = (WeightsJob*)calloc((size_t)num_threads, sizeof(WeightsJob));
+    th = (pthread_t*)calloc((size_t)num_threads, sizeof(pthread_t));
+    grids = (float**)calloc((size_t)num_threads, sizeof(float*));
+    if (!jobs || !th || !grids)
+    {
+        free(jobs); free(th); free(grids);
+        return -1.0;
+    }
+    pthread_barrier_init(&barrier, NULL, (unsigned)num_threads);
+    for (t = 0; t < num_threads; ++t)
+    {
+        WeightsJob* j = &jobs[t];
+        j->wfn = wfn;
+        j->rfn = rfn;
+        j->t = t;
+        j->num_threads = num_threads;
+        j->begin = (num_points * (size_t)t) / (size_t)num_threads;
+        j->end = (num_points * (size_t)(t + 1)) / (size_t)num_threads;
+        j->num_points = num_points;
+        j->cells = cells;
+        j->uu = uu; j->vv = vv; j->w_in = w_in; j->w_out = w_out;
+        j->cell_size_rad = cell_size_rad;
+        j->grid_size = grid_size;
+        j->grids = grids;
+        j->grid_out = grid_out;
+        j->barrier = &barrier;
+    }
+    for (t = 0; t < num_threads; ++t)
+        pthread_create(&th[t], NULL, weights_worker, &jobs[t]);
+    for (t = 0; t < num_threads; ++t) pthread_join(th[t], NULL);
+    pthread_barrier_destroy(&barrier);
+    *skipped_w = *skipped_r = 0;
+    for (t = 0; t < num_threads; ++t)
+    {
+        if (jobs[t].failed) worst = -1.0;
+        if (worst >= 0.0 && jobs[t].seconds > worst) worst = jobs[t].seconds;
+        *skipped_w += jobs[t].skipped_w;
+        *skipped_r += jobs[t].skipped_r;
+        free(jobs[t].grid);
+    }
+    free(jobs);
+    free(th);
+    free(grids);
+    return worst;
+}

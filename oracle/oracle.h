@@ -121,6 +121,20 @@ typedef void (*orc_grid_fn_f)(size_t, const int*, int, int, const float*,
         size_t, const float*, const float*, const float*, const float*,
         const float*, float, float, int, size_t*, double*, float*);
 
+typedef void (*orc_wwrite_fn_f)(size_t, const float*, const float*,
+        const float*, float, int, size_t*, float*);
+typedef void (*orc_wread_fn_f)(size_t, const float*, const float*,
+        const float*, float*, float, int, size_t*, const float*);
+
+/* Uniform-weighting CPU baseline (FP32): num_threads threads run wfn on
+ * contiguous slices into private grids, sum the private grids into
+ * grid_out in parallel (in thread order), then run rfn on the slices
+ * against grid_out.  Returns the seconds of the whole pass (or -1). */
+double orc_time_weights_parallel_f(orc_wwrite_fn_f wfn, orc_wread_fn_f rfn,
+        int num_threads, size_t num_points, const float* uu, const float* vv,
+        const float* w_in, float cell_size_rad, int grid_size,
+        float* grid_out, float* w_out, size_t* skipped_w, size_t* skipped_r);
+
 double orc_time_parallel_d(orc_grid_fn_d fn, int num_threads,
         size_t chunk_points, size_t num_w_planes, const int* support,
         int oversample, int conv_size_half, const double* conv_func,

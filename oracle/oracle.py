@@ -82,6 +82,10 @@ def oracle_lib():
             r = getattr(lib, "orc_grid_weights_read_" + t)
             r.argtypes = [_SZ, _P, _P, _P, _P, fa[0], C.c_int, _P, _P]
             w.restype = r.restype = None
+        lib.orc_time_weights_parallel_f.argtypes = [
+            _P, _P, C.c_int, _SZ, _P, _P, _P, C.c_float, C.c_int, _P, _P,
+            _P, _P]
+        lib.orc_time_weights_parallel_f.restype = C.c_double
         _oracle = lib
     return _oracle
 
@@ -212,6 +216,79 @@ def time_parallel(w: dict, single: bool, threads: int, use_reference: bool,
     if secs < 0:
         raise MemoryError("CPU baseline could not allocate private grids")
     return secs, skipped.value, nrm.value, out
+
+
+def weights(uu, vv, weight, cell_size_rad, grid_size, grid, weight_out,
+            single: bool = False, use_reference: bool = False):
+    """Uniform weighting as the reference's main loop does it: the weights
+    write (grid accumulates) then the read.  Arrays are copied, not
+    modified.  Returns (skipped_write, grid, skipped_read, weight_out)."""
+    sk_w, g, sk_r, wout, _ = weights_timed(uu, vv, weight, cell_size_rad,
+                                           grid_size, grid, weight_out,
+                                           single, use_reference)
+    return sk_w, g, sk_r, wout
+
+
+def weights_timed(uu, vv, weight, cell_size_rad, grid_size, grid, weight_out,
+                  single: bool = False, use_reference: bool = False):
+    """weights() that also returns the wall time of the write and read
+    calls themselves (seconds, one host thread; the functions are serial):
+    (skipped_write, grid, skipped_read, weight_out, (t_write, t_read))."""
+    import time
+    real = np.float32 if single else np.float64
+    t = "f" if single else "d"
+    lib = reference_lib() if use_reference else oracle_lib()
+    prefix = "ref_oskar_" if use_reference else "orc_"
+    a = [np.ascontiguousarray(x, dtype=real) for x in (uu, vv, weight)]
+    g = np.array(grid, dtype=real, copy=True)
+    wout = np.array(weight_out, dtype=real, copy=True)
+    n = a[0].size
+    sk_w = C.c_size_t(0)
+    sk_r = C.c_size_t(0)
+    cell = real(cell_size_rad)
+    t0 = time.perf_counter()
+    getattr(lib, prefix + "grid_weights_write_" + t)(
+        n, _ptr(a[0]), _ptr(a[1]), _ptr(a[2]), cell, grid_size,
+        C.byref(sk_w), _ptr(g))
+    t1 = time.perf_counter()
+    getattr(lib, prefix + "grid_weights_read_" + t)(
+        n, _ptr(a[0]), _ptr(a[1]), _ptr(a[2]), _ptr(wout), cell, grid_size,
+        C.byref(sk_r), _ptr(g))
+    t2 = time.perf_counter()
+    return sk_w.value, g, sk_r.value, wout, (t1 - t0, t2 - t1)
+
+
+def time_weights_parallel(uu, vv, weight, cell_size_rad, grid_size,
+                          threads: int, use_reference: bool):
+    """FP32 uniform weighting on `threads` host threads: the reference's
+    (use_reference) or the restated oskar_grid_weights_write_f on private
+    grids over slices, a parallel sum of the grids, then _read_f over
+    slices.  Returns (seconds, skipped_write, grid, skipped_read,
+    weight_out); the grid equals the serial one whenever its sums are exact
+    (e.g. unit weights)."""
+    a = [np.ascontiguousarray(x, dtype=np.float32) for x in (uu, vv, weight)]
+    n = a[0].size
+    grid = np.zeros(grid_size * grid_size, np.float32)
+    wout = np.zeros(n, np.float32)
+    if use_reference:
+        lib = reference_lib()
+        if lib is None:
+            raise RuntimeError("reference library not built (oracle/_ref)")
+        prefix = "ref_oskar_"
+    else:
+        lib = oracle_lib()
+        prefix = "orc_"
+    wfn = C.cast(getattr(lib, prefix + "grid_weights_write_f"), _P)
+    rfn = C.cast(getattr(lib, prefix + "grid_weights_read_f"), _P)
+    sk_w = C.c_size_t(0)
+    sk_r = C.c_size_t(0)
+    secs = oracle_lib().orc_time_weights_parallel_f(
+        wfn, rfn, threads, n, _ptr(a[0]), _ptr(a[1]), _ptr(a[2]),
+        np.float32(cell_size_rad), grid_size, _ptr(grid), _ptr(wout),
+        C.byref(sk_w), C.byref(sk_r))
+    if secs < 0:
+        raise MemoryError("CPU baseline could not allocate private grids")
+    return secs, sk_w.value, grid, sk_r.value, wout
 
 
 def rel_rms(test: np.ndarray, ref: np.ndarray) -> float:

@@ -18,8 +18,17 @@ def pytest_configure(config):
 
 
 def golden_names():
+    """Gridding fixtures (every fixture but the uniform-weighting ones)."""
     return sorted(os.path.splitext(os.path.basename(p))[0]
-                  for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz")))
+                  for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz"))
+                  if not os.path.basename(p).startswith("weights_"))
+
+
+def load_weights_golden(name):
+    """A uniform-weighting fixture: the reference's
+    oskar_grid_weights_write then _read on the stored inputs."""
+    z = np.load(os.path.join(GOLDEN_DIR, name + ".npz"))
+    return {k: z[k] for k in z.files}
 
 
 def load_golden(name):

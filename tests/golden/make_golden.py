@@ -126,6 +126,65 @@ def ones_inputs():
     return d
 
 
+def weights_inputs(seed=13):
+    """Uniform-weighting case (utils/oskar_grid_weights.c): grid_scale = 1
+    so positions are in cells; half-way positions, the first and last cell
+    of each axis and one past them, far-outside points, and a dense cluster
+    of points with non-integer weights so that many cells sum several
+    weights (their order matters).  The weights grid and weight_out start
+    from random values: the write accumulates and the read leaves skipped
+    points' outputs alone."""
+    rng = np.random.default_rng(seed)
+    g = 64
+    pts = []  # (u, v): pos_u = -u, pos_v = v
+    for u in (0.5, -0.5, 1.5, -1.5, 2.5, -2.5, 0.49999997, 0.50000003):
+        pts.append((u, -u))
+    for e in (32.0, 32.4, 32.5, -31.0, -31.4, -31.5, 1e9, -1e9):
+        pts.append((e, 0.0))
+        pts.append((0.0, -e))
+    n_rand = 3000
+    ru = rng.normal(0.0, 4.0, n_rand)
+    rv = rng.normal(0.0, 4.0, n_rand)
+    pts += list(zip(ru, rv))
+    a = np.array(pts, dtype=np.float64)
+    n = a.shape[0]
+    return dict(uu=a[:, 0].copy(), vv=a[:, 1].copy(),
+                weight=rng.uniform(0.1, 3.0, n), cell_size_rad=1.0 / g,
+                grid_size=g, grid=rng.uniform(0.0, 2.0, g * g),
+                weight_out=rng.uniform(-1.0, 1.0, n))
+
+
+def save_weights(name, inputs, single):
+    """Runs the reference's oskar_grid_weights_write then _read on the
+    inputs and stores inputs and outputs."""
+    import ctypes as C
+    ref = O.reference_lib()
+    if ref is None:
+        raise SystemExit("build oracle/_ref first (make -C oracle)")
+    real = np.float32 if single else np.float64
+    t = "f" if single else "d"
+    a = {k: np.ascontiguousarray(inputs[k], dtype=real)
+         for k in ("uu", "vv", "weight", "grid", "weight_out")}
+    cell = real(inputs["cell_size_rad"])
+    g = inputs["grid_size"]
+    n = a["uu"].size
+    grid = a["grid"].copy()
+    wout = a["weight_out"].copy()
+    sk_w = C.c_size_t(0)
+    sk_r = C.c_size_t(0)
+    getattr(ref, "ref_oskar_grid_weights_write_" + t)(
+        n, a["uu"].ctypes.data, a["vv"].ctypes.data, a["weight"].ctypes.data,
+        cell, g, C.byref(sk_w), grid.ctypes.data)
+    getattr(ref, "ref_oskar_grid_weights_read_" + t)(
+        n, a["uu"].ctypes.data, a["vv"].ctypes.data, a["weight"].ctypes.data,
+        wout.ctypes.data, cell, g, C.byref(sk_r), grid.ctypes.data)
+    np.savez_compressed(
+        os.path.join(OUT, name + ".npz"), cell_size_rad=np.asarray(cell),
+        grid_size=g, single=single, out_grid=grid, out_weight=wout,
+        out_skipped_write=sk_w.value, out_skipped_read=sk_r.value, **a)
+    print(f"{name}: n={n} skipped={sk_w.value}/{sk_r.value}")
+
+
 def save(name, inputs, single):
     ref = O.reference_lib()
     if ref is None:
@@ -155,6 +214,8 @@ def main():
     save("synth_small_d", synth_small_inputs(), single=False)
     save("synth_small_f", synth_small_inputs(), single=True)
     save("ones_d", ones_inputs(), single=False)
+    save_weights("weights_d", weights_inputs(), single=False)
+    save_weights("weights_f", weights_inputs(), single=True)
 
 
 if __name__ == "__main__":

@@ -116,8 +116,11 @@ def test_batch_can_be_graph_captured(oracle):
     graph = torch.cuda.CUDAGraph()
     with torch.cuda.graph(graph, stream=s):
         fg.grid_batch_device(ws, jobs, stream=s)
-    graph.replay()
-    graph.replay()
+    # torch replays a graph on the current stream: make that the stream the
+    # workspace's buffers are used on.
+    with torch.cuda.stream(s):
+        graph.replay()
+        graph.replay()
     torch.cuda.synchronize()
     for w, g in zip(wls, grids):
         if w.num_points == 0:

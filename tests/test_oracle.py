@@ -4,7 +4,7 @@ the golden fixtures generated from it."""
 import numpy as np
 import pytest
 
-from conftest import golden_names, load_golden
+from conftest import golden_names, load_golden, load_weights_golden
 from fpga_gridding_b200 import workloads as W
 
 
@@ -137,6 +137,53 @@ def test_weights_restatement_matches_reference(oracle, ref, small):
         assert outs[0][:2] == outs[1][:2]
         assert np.array_equal(outs[0][2], outs[1][2])
         assert np.array_equal(outs[0][3], outs[1][3])
+
+
+@pytest.mark.parametrize("name", ["weights_d", "weights_f"])
+def test_weights_oracle_matches_golden_bit_exact(oracle, name):
+    z = load_weights_golden(name)
+    sk_w, grid, sk_r, wout = oracle.weights(
+        z["uu"], z["vv"], z["weight"], z["cell_size_rad"], int(z["grid_size"]),
+        z["grid"], z["weight_out"], single=bool(z["single"]))
+    assert sk_w == int(z["out_skipped_write"])
+    assert sk_r == int(z["out_skipped_read"])
+    assert np.array_equal(grid, z["out_grid"])
+    assert np.array_equal(wout, z["out_weight"])
+    # Cells summing several non-integer weights are present, so the
+    # fixture pins the summation order.
+    cells = np.round(-z["uu"] * z["grid_size"] * z["cell_size_rad"])
+    assert np.unique(cells).size < cells.size // 4
+
+
+def test_weights_restatement_matches_reference_random_weights(oracle, ref,
+                                                              small):
+    rng = np.random.default_rng(21)
+    n = small["uu"].size
+    g = small["grid_size"]
+    for single in (False, True):
+        args = (small["uu"], small["vv"], rng.uniform(0.1, 2.0, n),
+                small["cell_size_rad"], g, rng.uniform(0, 1, g * g),
+                rng.uniform(-1, 1, n))
+        a = oracle.weights(*args, single=single)
+        b = oracle.weights(*args, single=single, use_reference=True)
+        assert a[0] == b[0] and a[2] == b[2]
+        assert np.array_equal(a[1], b[1]) and np.array_equal(a[3], b[3])
+
+
+def test_weights_parallel_harness_matches_serial_for_unit_weights(oracle,
+                                                                 small):
+    g = small["grid_size"]
+    n = small["uu"].size
+    ones = np.ones(n)
+    for use_ref in (False, True):
+        secs, sk_w, grid, sk_r, wout = oracle.time_weights_parallel(
+            small["uu"], small["vv"], ones, small["cell_size_rad"], g, 3,
+            use_ref)
+        s_w, g1, s_r, w1 = oracle.weights(
+            small["uu"], small["vv"], ones, small["cell_size_rad"], g,
+            np.zeros(g * g), np.zeros(n), single=True)
+        assert secs > 0 and (sk_w, sk_r) == (s_w, s_r)
+        assert np.array_equal(grid, g1) and np.array_equal(wout, w1)
 
 
 def test_parallel_timing_harness_sums_to_serial(oracle, small):
