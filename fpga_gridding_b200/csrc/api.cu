@@ -1,5 +1,6 @@
 // Public C ABI of the B200 gridder: the drop-in oskar_grid_wproj_{d,f}
 // replacements and the extended device-resident API.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -95,8 +96,12 @@ void workspace_free(oskar_B200Workspace* ws)
     if (!ws) return;
     DeviceGuard g(ws->device);
     if (ws->stream) cudaStreamSynchronize(ws->stream);
+    if (ws->copy_stream) cudaStreamSynchronize(ws->copy_stream);
     for (cudaEvent_t& e : ws->events)
         if (e) cudaEventDestroy(e);
+    for (cudaEvent_t& e : ws->ingest_events)
+        if (e) cudaEventDestroy(e);
+    if (ws->copy_stream) cudaStreamDestroy(ws->copy_stream);
     if (ws->jobs_event) cudaEventDestroy(ws->jobs_event);
     if (ws->h_jobs) cudaFreeHost(ws->h_jobs);
     if (ws->h_counters) cudaFreeHost(ws->h_counters);
@@ -221,15 +226,9 @@ int check_grid_args(size_t num_points, const void* uu, const void* vv,
     return OSKAR_B200_OK;
 }
 
-// Reads the device status word copied back by run_grid (after a sync).
-int device_check_status(const oskar_B200Workspace* ws)
-{
-    const unsigned long long s =
-        static_cast<const unsigned long long*>(ws->h_counters)[CNT_STATUS];
-    if (!s) return OSKAR_B200_OK;
-    if (s & DEV_ERR_TIMEOUT) return OSKAR_B200_ERR_TIMEOUT;
-    return OSKAR_B200_ERR_DEVICE_CHECK;
-}
+// Points per chunk of the drop-in's pipelined upload: chunk k is gridded
+// while chunk k + 1 crosses PCIe.
+constexpr size_t kIngestChunk = size_t(5) << 20;
 
 template <typename T>
 int drop_in(size_t num_w_planes, const int* support, int oversample,
@@ -267,65 +266,123 @@ int drop_in(size_t num_w_planes, const int* support, int oversample,
     const size_t cube_elems = num_w_planes * (size_t)conv_size_half *
                               conv_size_half * 2;
     const size_t grid_elems = 2 * (size_t)grid_size * grid_size;
+    const int chunks = n == 0 ? 1 : (int)std::min<size_t>(
+        kIngestEvents - 2, (n + kIngestChunk - 1) / kIngestChunk);
 #define B200_CHECK(expr)                                            \
     do {                                                            \
         const cudaError_t e_ = (expr);                              \
         if (e_ != cudaSuccess) { cudaStreamSynchronize(s);          \
+                                 if (ws->copy_stream)               \
+                                     cudaStreamSynchronize(         \
+                                         ws->copy_stream);          \
                                  cudaGetLastError();                \
                                  return status_from_cuda(e_); }     \
     } while (0)
+    // The uploads run on a second stream: the cube first, then the chunks
+    // of visibilities in order, then the caller's grid.  The gridding of
+    // chunk k waits only for chunk k, and it accumulates into a zeroed
+    // device grid, so the caller's grid crosses PCIe while the chunks grid;
+    // it is added in at the end.
+    if (!ws->copy_stream)
+        B200_CHECK(cudaStreamCreateWithFlags(&ws->copy_stream,
+                                             cudaStreamNonBlocking));
+    for (cudaEvent_t& e : ws->ingest_events)
+        if (!e) B200_CHECK(cudaEventCreateWithFlags(&e,
+                                                    cudaEventDisableTiming));
+    cudaStream_t c = ws->copy_stream;
+    cudaEvent_t ev_cube = ws->ingest_events[0];
+    cudaEvent_t ev_grid = ws->ingest_events[1];
+    cudaEvent_t* ev_chunk = ws->ingest_events + 2;
     B200_CHECK(ws->in_cube.ensure(cube_elems * sizeof(T)));
     B200_CHECK(ws->in_grid.ensure(grid_elems * sizeof(T)));
-    B200_CHECK(ws->in_norm.ensure(2 * sizeof(double)));
+    B200_CHECK(ws->acc_grid.ensure(grid_elems * sizeof(T)));
+    // [norm, device status of every chunk OR-ed, skip count of each chunk]
+    const size_t slots = 2 + (size_t)chunks;
+    B200_CHECK(ws->in_norm.ensure(sizeof(double) * slots));
     if (n)
     {
         B200_CHECK(ws->in_uu.ensure(n * sizeof(T)));
         B200_CHECK(ws->in_vv.ensure(n * sizeof(T)));
         B200_CHECK(ws->in_ww.ensure(n * sizeof(T)));
         B200_CHECK(ws->in_vis.ensure(2 * n * sizeof(T)));
-        B200_CHECK(cudaMemcpyAsync(ws->in_uu.ptr, uu, n * sizeof(T),
-                                   cudaMemcpyHostToDevice, s));
-        B200_CHECK(cudaMemcpyAsync(ws->in_vv.ptr, vv, n * sizeof(T),
-                                   cudaMemcpyHostToDevice, s));
-        B200_CHECK(cudaMemcpyAsync(ws->in_ww.ptr, ww, n * sizeof(T),
-                                   cudaMemcpyHostToDevice, s));
-        B200_CHECK(cudaMemcpyAsync(ws->in_vis.ptr, vis, 2 * n * sizeof(T),
-                                   cudaMemcpyHostToDevice, s));
     }
+    // The previous call's uploads were waited for before it returned.
     B200_CHECK(cudaMemcpyAsync(ws->in_cube.ptr, conv_func,
                                cube_elems * sizeof(T),
-                               cudaMemcpyHostToDevice, s));
-    B200_CHECK(cudaMemcpyAsync(ws->in_grid.ptr, grid, grid_elems * sizeof(T),
-                               cudaMemcpyHostToDevice, s));
-    B200_CHECK(cudaMemsetAsync(ws->in_norm.ptr, 0, 2 * sizeof(double), s));
+                               cudaMemcpyHostToDevice, c));
+    B200_CHECK(cudaEventRecord(ev_cube, c));
+    B200_CHECK(cudaStreamWaitEvent(s, ev_cube, 0));
     st = cube_init(tc.cube, device, num_w_planes, support, oversample,
                    conv_size_half, ws->in_cube.ptr, dbl, dbl,
                    OSKAR_B200_KERNEL_NATIVE, s);
-    if (st) { cudaStreamSynchronize(s); cudaGetLastError(); return st; }
+    if (st) { cudaStreamSynchronize(s); cudaStreamSynchronize(c);
+              cudaGetLastError(); return st; }
+    B200_CHECK(cudaMemsetAsync(ws->in_norm.ptr, 0, sizeof(double) * slots,
+                               s));
+    B200_CHECK(cudaMemsetAsync(ws->acc_grid.ptr, 0, grid_elems * sizeof(T),
+                               s));
     oskar_B200Options opt;
     oskar_b200_options_init(&opt);
     double* d_norm = static_cast<double*>(ws->in_norm.ptr);
-    unsigned long long* d_skip =
+    unsigned long long* d_status =
         reinterpret_cast<unsigned long long*>(d_norm + 1);
-    st = run_grid(ws, tc.cube, &opt, n, ws->in_uu.ptr, ws->in_vv.ptr,
-                  ws->in_ww.ptr, ws->in_vis.ptr, nullptr, cell_size_rad,
-                  w_scale, grid_size, ws->in_grid.ptr, d_skip, d_norm, s);
-    if (st) { cudaStreamSynchronize(s); cudaGetLastError(); return st; }
+    unsigned long long* d_skip = d_status + 1;
+    for (int k = 0; k < chunks; ++k)
+    {
+        const size_t b = n * (size_t)k / (size_t)chunks;
+        const size_t e = n * (size_t)(k + 1) / (size_t)chunks;
+        const size_t m = e - b;
+        T* du = static_cast<T*>(ws->in_uu.ptr) + b;
+        T* dv = static_cast<T*>(ws->in_vv.ptr) + b;
+        T* dw = static_cast<T*>(ws->in_ww.ptr) + b;
+        T* dz = static_cast<T*>(ws->in_vis.ptr) + 2 * b;
+        if (m)
+        {
+            B200_CHECK(cudaMemcpyAsync(du, uu + b, m * sizeof(T),
+                                       cudaMemcpyHostToDevice, c));
+            B200_CHECK(cudaMemcpyAsync(dv, vv + b, m * sizeof(T),
+                                       cudaMemcpyHostToDevice, c));
+            B200_CHECK(cudaMemcpyAsync(dw, ww + b, m * sizeof(T),
+                                       cudaMemcpyHostToDevice, c));
+            B200_CHECK(cudaMemcpyAsync(dz, vis + 2 * b, 2 * m * sizeof(T),
+                                       cudaMemcpyHostToDevice, c));
+        }
+        B200_CHECK(cudaEventRecord(ev_chunk[k], c));
+        B200_CHECK(cudaStreamWaitEvent(s, ev_chunk[k], 0));
+        st = run_grid(ws, tc.cube, &opt, m, du, dv, dw, dz, nullptr,
+                      cell_size_rad, w_scale, grid_size, ws->acc_grid.ptr,
+                      d_skip + k, d_norm, s);
+        if (st) { cudaStreamSynchronize(s); cudaStreamSynchronize(c);
+                  cudaGetLastError(); return st; }
+        // Each chunk resets the workspace's status word: keep its bits.
+        B200_CHECK(launch_status_or(ws, d_status, s));
+    }
+    B200_CHECK(cudaMemcpyAsync(ws->in_grid.ptr, grid, grid_elems * sizeof(T),
+                               cudaMemcpyHostToDevice, c));
+    B200_CHECK(cudaEventRecord(ev_grid, c));
+    B200_CHECK(cudaStreamWaitEvent(s, ev_grid, 0));
+    B200_CHECK(launch_add(ws->in_grid.ptr, ws->acc_grid.ptr, grid_elems,
+                          dbl, ws->num_sms, s));
     // Check the job before touching the caller's grid and norm.
     B200_CHECK(cudaStreamSynchronize(s));
+    B200_CHECK(cudaStreamSynchronize(c));
     B200_CHECK(cudaGetLastError());
-    st = device_check_status(ws);
-    if (st) return st;
-    double out[2];
-    B200_CHECK(cudaMemcpyAsync(out, d_norm, sizeof(out),
+    std::vector<unsigned long long> out(slots);
+    B200_CHECK(cudaMemcpyAsync(out.data(), d_norm,
+                               sizeof(double) * slots,
                                cudaMemcpyDeviceToHost, s));
+    B200_CHECK(cudaStreamSynchronize(s));
+    if (out[1]) return out[1] & DEV_ERR_TIMEOUT ? OSKAR_B200_ERR_TIMEOUT
+                                                : OSKAR_B200_ERR_DEVICE_CHECK;
     B200_CHECK(cudaMemcpyAsync(grid, ws->in_grid.ptr, grid_elems * sizeof(T),
                                cudaMemcpyDeviceToHost, s));
     B200_CHECK(cudaStreamSynchronize(s));
 #undef B200_CHECK
-    unsigned long long skipped;
-    memcpy(&skipped, &out[1], sizeof(skipped));
-    *norm += out[0];
+    unsigned long long skipped = 0;
+    for (int k = 0; k < chunks; ++k) skipped += out[2 + k];
+    double nrm;
+    memcpy(&nrm, &out[0], sizeof(nrm));
+    *norm += nrm;
     *num_skipped = (size_t)skipped;
     return OSKAR_B200_OK;
 }

@@ -85,6 +85,9 @@ struct DeviceBuffer
     }
 };
 
+// Events of the drop-in's pipelined upload: cube, grid and up to 14 chunks.
+constexpr int kIngestEvents = 16;
+
 // Grid-launch tuning for one support size (the "autotuner" table entry).
 struct TuneEntry
 {
@@ -117,6 +120,11 @@ struct oskar_B200Workspace
         in_cube, in_norm;
     // error grid of ACCUM_COMPENSATED
     b200::DeviceBuffer comp_grid;
+    // drop-in pipelined upload: copy stream, its events (cube, grid, one per
+    // chunk) and the zeroed grid the chunks accumulate into
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ingest_events[b200::kIngestEvents] = {};
+    b200::DeviceBuffer acc_grid;
     // pinned host mirror of the device counters (stats)
     void* h_counters = nullptr;
     unsigned long long last_points = 0;
@@ -251,6 +259,13 @@ int run_weights_read(oskar_B200Workspace* ws, int data_is_double, size_t n,
 
 int selftest_bounded_wait(oskar_B200Workspace* ws, unsigned spins,
                           int* device_status);
+
+// dst[i] += src[i] for n reals (FP64 when is_double, else FP32).
+cudaError_t launch_add(void* dst, const void* src, size_t n, int is_double,
+                       int num_sms, cudaStream_t st);
+// *acc |= the workspace's device status word (after a run_batch on st).
+cudaError_t launch_status_or(oskar_B200Workspace* ws,
+                             unsigned long long* acc, cudaStream_t st);
 
 int status_from_cuda(cudaError_t e);
 

@@ -394,7 +394,45 @@ __global__ void bounded_wait_probe_kernel(unsigned spins,
         atomicOr(status, (unsigned long long)DEV_ERR_TIMEOUT);
 }
 
+template <typename T>
+__global__ void add_kernel(T* __restrict__ dst, const T* __restrict__ src,
+                           size_t n)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        dst[i] += src[i];
+}
+
+__global__ void status_or_kernel(const unsigned long long* counters,
+                                 unsigned long long* acc)
+{
+    if (counters[CNT_STATUS]) *acc |= counters[CNT_STATUS];
+}
+
 }  // namespace
+
+cudaError_t launch_add(void* dst, const void* src, size_t n, int is_double,
+                       int num_sms, cudaStream_t st)
+{
+    if (n == 0) return cudaSuccess;
+    const size_t want = (n + 255) / 256, cap = (size_t)num_sms * 8;
+    const unsigned blocks = (unsigned)(want < cap ? want : cap);
+    if (is_double)
+        add_kernel<double><<<blocks, 256, 0, st>>>(
+            static_cast<double*>(dst), static_cast<const double*>(src), n);
+    else
+        add_kernel<float><<<blocks, 256, 0, st>>>(
+            static_cast<float*>(dst), static_cast<const float*>(src), n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_status_or(oskar_B200Workspace* ws,
+                             unsigned long long* acc, cudaStream_t st)
+{
+    status_or_kernel<<<1, 1, 0, st>>>(
+        static_cast<const unsigned long long*>(ws->counters.ptr), acc);
+    return cudaGetLastError();
+}
 
 int selftest_bounded_wait(oskar_B200Workspace* ws, unsigned spins,
                           int* device_status)

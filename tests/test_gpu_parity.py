@@ -80,6 +80,45 @@ def test_dropin_accumulates_into_grid_and_norm(oracle, small):
     assert abs(n2 - n1) <= TOL_D * abs(n1)
 
 
+def _many_points(n, seed=12):
+    """n random visibilities on a 512^2 grid with supports 1 -> 3: enough
+    points that the drop-in uploads and grids them in several chunks."""
+    rng = np.random.default_rng(seed)
+    g, os_ = 512, 4
+    support = W.support_ramp(8, 1, 3)
+    csh = W.min_conv_size_half(support, os_) + 1
+    cube = W.analytic_kernel_cube(support, os_, csh).numpy()
+    pos = rng.uniform(-240.0, 240.0, (2, n))
+    return dict(num_w_planes=8, support=support, oversample=os_,
+                conv_size_half=csh, conv_func=cube, uu=-pos[0] / g,
+                vv=pos[1] / g, ww=rng.uniform(-49.0, 49.0, n),
+                vis=rng.normal(size=2 * n), weight=np.ones(n),
+                cell_size_rad=1.0, w_scale=1.0, grid_size=g)
+
+
+@pytest.mark.parametrize("single", [False, True])
+def test_dropin_pipelined_chunks(oracle, single):
+    """5.6 M points: the drop-in uploads them in chunks that are gridded
+    while the next chunk and the caller's grid cross PCIe; the result
+    matches the oracle as one call does."""
+    w = _many_points(5_600_000)
+    g = w["grid_size"]
+    rng = np.random.default_rng(2)
+    real = np.float32 if single else np.float64
+    base = rng.normal(size=2 * g * g).astype(real)
+    ref_in = promote(w) if single else w
+    s1, n1, g1 = oracle.grid_d(ref_in, grid_arr=base.astype(np.float64),
+                               norm=1.25, threads=8)
+    s2, n2, g2 = fg.grid_workload(w, single=single, grid=base.copy(),
+                                  norm=1.25)
+    assert s1 == s2
+    assert oracle.rel_rms(g2, g1) <= (TOL_F if single else TOL_D)
+    # norm is a sum of 5.6 M positive FP64 terms: the reference adds them
+    # one by one, the GPU in per-block partials; the two orders may differ
+    # by up to n * 2^-53 relative.
+    assert abs(n2 - n1) <= max(TOL_D, w["uu"].size * 2.0 ** -53) * abs(n1)
+
+
 @pytest.mark.parametrize("name", golden_names())
 def test_golden_fixtures(name):
     inputs, out = load_golden(name)
