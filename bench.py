@@ -292,6 +292,13 @@ def run_b200(args, world, rank, local):
     torch.cuda.synchronize()
     clk = clocks.stop()
     elapsed_ms = ev0.elapsed_time(ev1)
+    # One more (untimed) step with the grid atomics counted: counting costs
+    # an instruction per tap, so the timed steps run without it.
+    lib.oskar_b200_set_stage_timing(ws.handle, 3)
+    step()
+    stream.synchronize()
+    issued_atomics = ws.stats().atomic_flushes
+    lib.oskar_b200_set_stage_timing(ws.handle, 1)
     barrier(world)
     elapsed_ms = max_over_ranks(elapsed_ms, world)
     ms_per_step = elapsed_ms / args.steps
@@ -325,9 +332,9 @@ def run_b200(args, world, rank, local):
     l2_atomic = {"peak_red_v2_per_s": rate.value,
                  "grid_updates_per_s_in_kernel": kernel_updates_per_s,
                  "frac": round(kernel_updates_per_s / rate.value, 4),
-                 "issued_atomics_per_launch": stats.atomic_flushes,
+                 "issued_atomics_per_launch": issued_atomics,
                  "issued_atomic_frac": round(
-                     stats.atomic_flushes / (kernel_ms * 1e-3) / rate.value, 4)}
+                     issued_atomics / (kernel_ms * 1e-3) / rate.value, 4)}
     stage_ms = {"prep": round(stats.prep_ms, 3), "sort": round(stats.sort_ms, 3),
                 "permute_tasks": round(stats.tasks_ms, 3),
                 "grid": round(stats.grid_ms, 3)}

@@ -684,7 +684,7 @@ int oskar_b200_set_stage_timing(oskar_B200Workspace* ws, int enable)
                 const cudaError_t r = cudaEventCreate(&e);
                 if (r != cudaSuccess) return status_from_cuda(r);
             }
-    ws->stage_timing = enable ? 1 : 0;
+    ws->stage_timing = enable & 3;
     ws->events_recorded = 0;
     return OSKAR_B200_OK;
 }

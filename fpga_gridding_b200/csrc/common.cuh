@@ -114,14 +114,17 @@ template <typename KT> struct KernelLoad;
 
 template <> struct KernelLoad<float2>
 {
+    using Wide = float2;
     __device__ __forceinline__ static float2 get(const float2& k) { return k; }
 };
 template <> struct KernelLoad<double2>
 {
+    using Wide = double2;
     __device__ __forceinline__ static double2 get(const double2& k) { return k; }
 };
 template <> struct KernelLoad<__half2>
 {
+    using Wide = float2;
     __device__ __forceinline__ static float2 get(const __half2& k)
     {
         return __half22float2(k);
@@ -129,6 +132,7 @@ template <> struct KernelLoad<__half2>
 };
 template <> struct KernelLoad<__nv_bfloat162>
 {
+    using Wide = float2;
     __device__ __forceinline__ static float2 get(const __nv_bfloat162& k)
     {
         return __bfloat1622float2(k);

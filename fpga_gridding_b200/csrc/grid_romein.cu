@@ -250,14 +250,18 @@ struct CompensatedFlush
 };
 
 // One task: every class of the W x W footprint over the task's visibilities.
-template <typename GT, typename KT, int CPT, typename FL>
+// Each class keeps a running sum for its current cell and flushes it when
+// the cell changes (and at the end).  Every cell a class visits lies inside
+// the grid: the prep kernel keeps only footprints inside the grid, derive()
+// moves a record that breaks this to cell 0 with zero weight, and tasks
+// whose footprint is wider than the grid are rejected before this point.
+template <typename GT, typename KT, int CPT, bool COUNT, typename FL>
 __device__ __forceinline__ void process_task(const TapVis<GT>* __restrict__ s_vis,
                                              int m, int w, int pitch,
                                              int row_shift,
                                              const KT* __restrict__ slab,
                                              const FL& flush,
-                                             int grid_size, unsigned cells,
-                                             unsigned& flushes)
+                                             int grid_size, unsigned& flushes)
 {
     const TaskLayout lay = task_layout<CPT>(w);
     const int per_slice = w * lay.groups;
@@ -272,15 +276,24 @@ __device__ __forceinline__ void process_task(const TapVis<GT>* __restrict__ s_vi
         const int b0 = pass * lay.groups * CPT + g;
         GT are[CPT], aim[CPT];
         unsigned cur[CPT];
-#pragma unroll
-        for (int q = 0; q < CPT; ++q)
-        {
-            are[q] = aim[q] = GT(0);
-            cur[q] = 0xffffffffu;
-        }
         // Rows of this thread in this pass: b0 + q * groups, q < rows_here.
         int rows_here = (w - b0 + lay.groups - 1) / lay.groups;
         rows_here = rows_here < 0 ? 0 : (rows_here > CPT ? CPT : rows_here);
+        {
+            // The first visibility's cells: its taps flush nothing.
+            const TapVis<GT> v = s_vis[i0];
+            const unsigned ru = min((unsigned)(a + v.mu),
+                                    (unsigned)(a + v.mu - w));
+#pragma unroll
+            for (int q = 0; q < CPT; ++q)
+            {
+                const int b = b0 + q * lay.groups;
+                const unsigned rv = min((unsigned)(b + v.mv),
+                                        (unsigned)(b + v.mv - w));
+                cur[q] = v.origin + ru + rv * (unsigned)grid_size;
+                are[q] = aim[q] = GT(0);
+            }
+        }
         for (int i = i0; i < i1; ++i)
         {
             const TapVis<GT> v = s_vis[i];
@@ -290,20 +303,28 @@ __device__ __forceinline__ void process_task(const TapVis<GT>* __restrict__ s_vi
             const int col = (int)ru >= v.tu ? v.cp + (int)ru : v.cn - (int)ru;
             const int kbase = v.rowbase - row_shift + col;
             const unsigned cell0 = v.origin + ru;
+            // All of this visibility's kernel values for the thread's rows
+            // are requested before any is used (predicated, not branched).
+            unsigned rvs[CPT];
+            typename KernelLoad<KT>::Wide kv[CPT];
+#pragma unroll
+            for (int q = 0; q < CPT; ++q)
+            {
+                const int b = b0 + q * lay.groups;
+                rvs[q] = min((unsigned)(b + v.mv), (unsigned)(b + v.mv - w));
+                KT raw{};
+                if (q < rows_here) raw = slab[kbase + (int)rvs[q] * pitch];
+                kv[q] = KernelLoad<KT>::get(raw);
+            }
 #pragma unroll
             for (int q = 0; q < CPT; ++q)
             {
                 if (q >= rows_here) break;
-                const int b = b0 + q * lay.groups;
-                const unsigned rv = min((unsigned)(b + v.mv),
-                                        (unsigned)(b + v.mv - w));
-                const auto k = KernelLoad<KT>::get(
-                    slab[kbase + (int)rv * pitch]);
-                const unsigned cell = cell0 + rv * (unsigned)grid_size;
+                const auto k = kv[q];
+                const unsigned cell = cell0 + rvs[q] * (unsigned)grid_size;
                 const bool change = cell != cur[q];
-                // cur = 0xffffffff (no cell yet) is >= cells: nothing to add.
-                flush(change && cur[q] < cells, cur[q], are[q], aim[q]);
-                flushes += change;
+                flush(change, cur[q], are[q], aim[q]);
+                if (COUNT) flushes += change;
                 are[q] = change ? GT(0) : are[q];
                 aim[q] = change ? GT(0) : aim[q];
                 cur[q] = cell;
@@ -315,20 +336,24 @@ __device__ __forceinline__ void process_task(const TapVis<GT>* __restrict__ s_vi
         }
 #pragma unroll
         for (int q = 0; q < CPT; ++q)
-            flush(cur[q] < cells, cur[q], are[q], aim[q]);
+        {
+            if (q >= rows_here) break;
+            flush(true, cur[q], are[q], aim[q]);
+        }
+        if (COUNT) flushes += rows_here > 0 ? rows_here : 0;
     }
 }
 
-template <typename GT, typename KT, typename FL>
+template <typename GT, typename KT, bool COUNT, typename FL>
 __device__ __forceinline__ void dispatch_cpt(int cpt, const TapVis<GT>* s_vis,
                                              int m, int w, int pitch,
                                              int row_shift, const KT* slab,
                                              const FL& fl, int grid_size,
-                                             unsigned cells, unsigned& flushes)
+                                             unsigned& flushes)
 {
 #define B200_CPT(C)                                                         \
-    process_task<GT, KT, C, FL>(s_vis, m, w, pitch, row_shift, slab, fl,    \
-                                grid_size, cells, flushes)
+    process_task<GT, KT, C, COUNT, FL>(s_vis, m, w, pitch, row_shift, slab,\
+                                       fl, grid_size, flushes)
     switch (cpt)
     {
     case 1: B200_CPT(1); break;
@@ -366,8 +391,10 @@ __device__ __forceinline__ CompensatedFlush make_flush<float, true>(void* grid, 
                             active};
 }
 
-template <typename GT, typename KT, bool STAGED, bool COMP>
-__global__ void __launch_bounds__(kGridThreads)
+// At least 3 CTAs per SM (<= 85 registers): measured faster on plain_large
+// than 4 CTAs with spills or 2 CTAs unconstrained.
+template <typename GT, typename KT, bool STAGED, bool COMP, bool COUNT>
+__global__ void __launch_bounds__(kGridThreads, 3)
 romein_grid_kernel(const GridArgs a)
 {
     using V2 = typename Vec2<GT>::type;
@@ -431,11 +458,18 @@ romein_grid_kernel(const GridArgs a)
         }
         const auto fl = make_flush<GT, COMP>(jd.grid, jd.comp, comp_here);
         const int grid_size = jd.grid_size;
-        const unsigned cells = (unsigned)grid_size * (unsigned)grid_size;
         const int offsets = 2 * jd.half + 1;
         const int plane = a.srec[begin].z & 0x7fffffff;
         const PlaneDesc d = static_cast<const PlaneDesc*>(jd.planes)[plane];
         const int w = 2 * d.support + 1;
+        // No kept footprint is wider than its grid; a task that says
+        // otherwise is malformed (and its cells could leave the grid).
+        if (w > grid_size)
+        {
+            if (threadIdx.x == 0)
+                atomicOr(status, (unsigned long long)DEV_ERR_TASK);
+            continue;
+        }
         const int cpt = d.support < kTuneMax ? a.cpt[d.support] : 5;
 
         // Order the task's visibilities by (row offset, cell): each run of
@@ -463,9 +497,9 @@ romein_grid_kernel(const GridArgs a)
 
         if (!STAGED)
         {
-            dispatch_cpt<GT, KT>(cpt, s_vis, m, w, d.pitch, 0,
-                                 slabs + d.offset, fl, grid_size, cells,
-                                 flushes);
+            dispatch_cpt<GT, KT, COUNT>(cpt, s_vis, m, w, d.pitch, 0,
+                                        slabs + d.offset, fl, grid_size,
+                                        flushes);
             continue;
         }
         const unsigned block_elems = (unsigned)w * (unsigned)d.pitch;
@@ -497,22 +531,26 @@ romein_grid_kernel(const GridArgs a)
                 return;
             }
             phase ^= 1u;
-            dispatch_cpt<GT, KT>(cpt, s_vis + rb, re - rb, w, d.pitch,
-                                 ov * (int)block_elems, s_block, fl,
-                                 grid_size, cells, flushes);
+            dispatch_cpt<GT, KT, COUNT>(cpt, s_vis + rb, re - rb, w,
+                                        d.pitch, ov * (int)block_elems,
+                                        s_block, fl, grid_size, flushes);
             __syncthreads();
         }
     }
-    const unsigned long long f = warp_sum((unsigned long long)flushes);
-    if ((threadIdx.x & 31) == 0 && f)
-        atomicAdd(&a.counters[CNT_FLUSHES], f);
+    if (COUNT)
+    {
+        const unsigned long long f = warp_sum((unsigned long long)flushes);
+        if ((threadIdx.x & 31) == 0 && f)
+            atomicAdd(&a.counters[CNT_FLUSHES], f);
+    }
 }
 
-template <typename GT, typename KT, bool STAGED, bool COMP = false>
+template <typename GT, typename KT, bool STAGED, bool COMP = false,
+          bool COUNT = false>
 cudaError_t launch_variant(const GridArgs& a, int num_sms, size_t smem,
                            cudaStream_t st, int* ctas_out)
 {
-    auto fn = romein_grid_kernel<GT, KT, STAGED, COMP>;
+    auto fn = romein_grid_kernel<GT, KT, STAGED, COMP, COUNT>;
     // Function attributes and occupancy are looked up once per (variant,
     // device, shared-memory size), not on every launch.
     static std::mutex mu;
@@ -657,31 +695,43 @@ cudaError_t launch_grid(const GridArgs& a, int data_is_double,
         switch (kernel_type)
         {
         case OSKAR_B200_KERNEL_F16:
-            return launch_variant<float, __half2, false, true>(args, num_sms, smem, st, ctas_out);
+            return a.count_flushes
+                ? launch_variant<float, __half2, false, true, true>(args, num_sms, smem, st, ctas_out)
+                : launch_variant<float, __half2, false, true>(args, num_sms, smem, st, ctas_out);
         case OSKAR_B200_KERNEL_BF16:
-            return launch_variant<float, __nv_bfloat162, false, true>(args, num_sms, smem, st, ctas_out);
+            return a.count_flushes
+                ? launch_variant<float, __nv_bfloat162, false, true, true>(args, num_sms, smem, st, ctas_out)
+                : launch_variant<float, __nv_bfloat162, false, true>(args, num_sms, smem, st, ctas_out);
         default:
-            return launch_variant<float, float2, false, true>(args, num_sms, smem, st, ctas_out);
+            return a.count_flushes
+                ? launch_variant<float, float2, false, true, true>(args, num_sms, smem, st, ctas_out)
+                : launch_variant<float, float2, false, true>(args, num_sms, smem, st, ctas_out);
         }
     }
+    // Flushes are counted (statistics) on the L1 path only.
+    const bool count = a.count_flushes && !staged;
     if (data_is_double)
     {
         if (kernel_type != OSKAR_B200_KERNEL_NATIVE)
             return cudaErrorInvalidValue;
-        return staged ? launch_variant<double, double2, true>(args, num_sms, smem, st, ctas_out)
-                      : launch_variant<double, double2, false>(args, num_sms, smem, st, ctas_out);
+        if (staged) return launch_variant<double, double2, true>(args, num_sms, smem, st, ctas_out);
+        return count ? launch_variant<double, double2, false, false, true>(args, num_sms, smem, st, ctas_out)
+                     : launch_variant<double, double2, false>(args, num_sms, smem, st, ctas_out);
     }
     switch (kernel_type)
     {
     case OSKAR_B200_KERNEL_F16:
-        return staged ? launch_variant<float, __half2, true>(args, num_sms, smem, st, ctas_out)
-                      : launch_variant<float, __half2, false>(args, num_sms, smem, st, ctas_out);
+        if (staged) return launch_variant<float, __half2, true>(args, num_sms, smem, st, ctas_out);
+        return count ? launch_variant<float, __half2, false, false, true>(args, num_sms, smem, st, ctas_out)
+                     : launch_variant<float, __half2, false>(args, num_sms, smem, st, ctas_out);
     case OSKAR_B200_KERNEL_BF16:
-        return staged ? launch_variant<float, __nv_bfloat162, true>(args, num_sms, smem, st, ctas_out)
-                      : launch_variant<float, __nv_bfloat162, false>(args, num_sms, smem, st, ctas_out);
+        if (staged) return launch_variant<float, __nv_bfloat162, true>(args, num_sms, smem, st, ctas_out);
+        return count ? launch_variant<float, __nv_bfloat162, false, false, true>(args, num_sms, smem, st, ctas_out)
+                     : launch_variant<float, __nv_bfloat162, false>(args, num_sms, smem, st, ctas_out);
     default:
-        return staged ? launch_variant<float, float2, true>(args, num_sms, smem, st, ctas_out)
-                      : launch_variant<float, float2, false>(args, num_sms, smem, st, ctas_out);
+        if (staged) return launch_variant<float, float2, true>(args, num_sms, smem, st, ctas_out);
+        return count ? launch_variant<float, float2, false, false, true>(args, num_sms, smem, st, ctas_out)
+                     : launch_variant<float, float2, false>(args, num_sms, smem, st, ctas_out);
     }
 }
 

@@ -21,6 +21,7 @@ struct GridArgs
     unsigned long long* counters;
     unsigned block_smem_bytes;  // set by launch_grid
     int comp_radius;            // see oskar_B200Options::compensate_radius
+    int count_flushes;          // count grid atomics (statistics)
     unsigned char cpt[kTuneMax];
 };
 

@@ -129,7 +129,8 @@ struct oskar_B200Workspace
     void* h_counters = nullptr;
     unsigned long long last_points = 0;
     int last_launches = 0;
-    // stage timing (oskar_b200_set_stage_timing)
+    // statistics level (oskar_b200_set_stage_timing): bit 0 stage events,
+    // bit 1 atomic counting
     int stage_timing = 0;
     int events_recorded = 0;
     cudaEvent_t events[5] = {};

@@ -308,7 +308,8 @@ typedef struct oskar_B200Stats
     unsigned long long num_gridded;    /* not skipped */
     unsigned long long grid_updates;   /* sum of (2S+1)^2 over gridded */
     unsigned long long num_tasks;      /* gridding work items */
-    unsigned long long atomic_flushes; /* grid atomics issued */
+    unsigned long long atomic_flushes; /* grid atomics issued (counted only
+                                          with statistics level bit 1) */
     int status;                        /* device-side check status */
     int kernel_launches;               /* kernels the call launched */
     /* Stage durations in ms (CUDA events on the call's stream), filled
@@ -320,8 +321,11 @@ typedef struct oskar_B200Stats
 OSKAR_B200_EXPORT int oskar_b200_last_stats(oskar_B200Workspace* ws,
         oskar_B200Stats* stats);
 
-/* Records CUDA events between the stages of every later oskar_b200_grid
- * call on this workspace (enable = 1) or stops doing so (0). */
+/* Statistics level of every later gridding call on this workspace:
+ * 0 = none; bit 0 (1) = CUDA events between the stages (stage times in
+ * oskar_B200Stats); bit 1 (2) = also count the grid atomics the gridding
+ * kernel issues (atomic_flushes; costs an instruction per tap, so leave it
+ * off when timing). */
 OSKAR_B200_EXPORT int oskar_b200_set_stage_timing(oskar_B200Workspace* ws,
         int enable);
 

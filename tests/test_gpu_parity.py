@@ -265,7 +265,15 @@ def test_stats_count_grid_updates(ws, oracle, small):
     _, _, _, st = _grid_ext(ws, small, True)
     assert st.grid_updates == oracle.count_taps(small)
     assert st.num_gridded == len(small["uu"])
+    assert st.atomic_flushes == 0  # not counted unless asked for
+    # statistics level 3: stage events and the grid atomics counted
+    ws._lib.oskar_b200_set_stage_timing(ws.handle, 3)
+    try:
+        _, _, _, st = _grid_ext(ws, small, True)
+    finally:
+        ws._lib.oskar_b200_set_stage_timing(ws.handle, 0)
     assert 0 < st.atomic_flushes < st.grid_updates
+    assert st.grid_ms > 0
 
 
 def test_compensated_accumulation(ws, oracle, small):
