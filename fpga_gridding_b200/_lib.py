@@ -32,6 +32,10 @@ EXPORTED_SYMBOLS = (
     "oskar_b200_place",
     "oskar_b200_weights_write",
     "oskar_b200_weights_read",
+    "oskar_b200_blocks_create",
+    "oskar_b200_blocks_push",
+    "oskar_b200_blocks_finish",
+    "oskar_b200_blocks_free",
     "oskar_b200_last_stats",
     "oskar_b200_set_stage_timing",
     "oskar_b200_measure_atomic_rate",
@@ -71,7 +75,8 @@ class Options(C.Structure):
     _fields_ = [("coord_mode", C.c_int), ("kernel_type", C.c_int),
                 ("accum_mode", C.c_int), ("apply_weight", C.c_int),
                 ("classes_per_thread", C.c_int), ("staging", C.c_int),
-                ("compensate_radius", C.c_int), ("reserved", C.c_int * 9)]
+                ("compensate_radius", C.c_int), ("reserved0", C.c_int),
+                ("frequency_hz", C.c_double), ("reserved", C.c_int * 6)]
 
 
 class Stats(C.Structure):
@@ -93,7 +98,8 @@ class Request(C.Structure):
     _fields_ = [("tag", C.c_ulonglong), ("cube", _P), ("num_points", _SZ),
                 ("uu", _P), ("vv", _P), ("ww", _P), ("vis", _P),
                 ("weight", _P), ("cell_size_rad", C.c_double),
-                ("w_scale", C.c_double), ("grid_size", C.c_int)]
+                ("w_scale", C.c_double), ("grid_size", C.c_int),
+                ("frequency_hz", C.c_double)]
 
 
 class Completion(C.Structure):
@@ -111,7 +117,7 @@ class Job(C.Structure):
                 ("ww", _P), ("vis", _P), ("weight", _P),
                 ("cell_size_rad", C.c_double), ("w_scale", C.c_double),
                 ("grid_size", C.c_int), ("grid", _P), ("d_num_skipped", _P),
-                ("d_norm", _P)]
+                ("d_norm", _P), ("frequency_hz", C.c_double)]
 
 
 def load():
@@ -139,9 +145,17 @@ def load():
         fr.restype = None
     lib.oskar_b200_weights_write.argtypes = [
         _P, C.c_int, C.c_int, _SZ, _P, _P, _P, C.c_double, C.c_int, _P, _P,
-        _P]
+        C.c_double, _P]
     lib.oskar_b200_weights_read.argtypes = [
-        _P, C.c_int, _SZ, _P, _P, _P, _P, C.c_double, C.c_int, _P, _P, _P]
+        _P, C.c_int, _SZ, _P, _P, _P, _P, C.c_double, C.c_int, _P, _P,
+        C.c_double, _P]
+    lib.oskar_b200_blocks_create.argtypes = [
+        _P, _P, C.POINTER(Options), C.c_double, C.c_double, C.c_int, _P, _P,
+        C.POINTER(_P)]
+    lib.oskar_b200_blocks_push.argtypes = [_P, _SZ, _P, _P, _P, _P, _P,
+                                           C.c_double]
+    lib.oskar_b200_blocks_finish.argtypes = [_P, C.POINTER(C.c_ulonglong)]
+    lib.oskar_b200_blocks_free.argtypes = [_P]
     lib.oskar_grid_wproj_b200_last_error.restype = C.c_int
     lib.oskar_grid_wproj_b200_error_string.argtypes = [C.c_int]
     lib.oskar_grid_wproj_b200_error_string.restype = C.c_char_p

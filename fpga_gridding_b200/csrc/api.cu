@@ -1,6 +1,7 @@
 // Public C ABI of the B200 gridder: the drop-in oskar_grid_wproj_{d,f}
 // replacements and the extended device-resident API.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -194,23 +195,6 @@ int cube_init(oskar_B200Cube* c, int device, size_t num_w_planes,
     return cube_build(c, d_conv, conv_is_double, st);
 }
 
-int check_options(const oskar_B200Options* opt, int data_is_double)
-{
-    if (opt->coord_mode != OSKAR_B200_COORDS_F64 &&
-        opt->coord_mode != OSKAR_B200_COORDS_REFERENCE_F32)
-        return OSKAR_B200_ERR_INVALID_ARGUMENT;
-    if (data_is_double && opt->coord_mode != OSKAR_B200_COORDS_F64)
-        return OSKAR_B200_ERR_UNSUPPORTED;
-    if (opt->accum_mode != OSKAR_B200_ACCUM_PLAIN &&
-        opt->accum_mode != OSKAR_B200_ACCUM_COMPENSATED)
-        return OSKAR_B200_ERR_INVALID_ARGUMENT;
-    if (opt->accum_mode == OSKAR_B200_ACCUM_COMPENSATED &&
-        (data_is_double || opt->staging == 1))
-        return OSKAR_B200_ERR_UNSUPPORTED;
-    if (opt->staging < 0 || opt->staging > 2)
-        return OSKAR_B200_ERR_INVALID_ARGUMENT;
-    return OSKAR_B200_OK;
-}
 
 int check_grid_args(size_t num_points, const void* uu, const void* vv,
                     const void* ww, const void* vis, const void* weight,
@@ -388,6 +372,30 @@ int drop_in(size_t num_w_planes, const int* support, int oversample,
 }
 
 }  // namespace
+
+namespace b200 {
+
+int check_options(const oskar_B200Options* opt, int data_is_double)
+{
+    if (opt->coord_mode != OSKAR_B200_COORDS_F64 &&
+        opt->coord_mode != OSKAR_B200_COORDS_REFERENCE_F32)
+        return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    if (data_is_double && opt->coord_mode != OSKAR_B200_COORDS_F64)
+        return OSKAR_B200_ERR_UNSUPPORTED;
+    if (opt->accum_mode != OSKAR_B200_ACCUM_PLAIN &&
+        opt->accum_mode != OSKAR_B200_ACCUM_COMPENSATED)
+        return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    if (opt->accum_mode == OSKAR_B200_ACCUM_COMPENSATED &&
+        (data_is_double || opt->staging == 1))
+        return OSKAR_B200_ERR_UNSUPPORTED;
+    if (opt->staging < 0 || opt->staging > 2)
+        return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    if (!(opt->frequency_hz >= 0.0) || !std::isfinite(opt->frequency_hz))
+        return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    return OSKAR_B200_OK;
+}
+
+}  // namespace b200
 
 // ---------------------------------------------------------------------------
 // Drop-in entry points
@@ -598,9 +606,12 @@ int oskar_b200_grid_batch(oskar_B200Workspace* ws,
                              in.weight, opt->apply_weight, in.grid_size,
                              in.grid);
         if (st) return st;
+        if (!(in.frequency_hz >= 0.0) || !std::isfinite(in.frequency_hz))
+            return OSKAR_B200_ERR_INVALID_ARGUMENT;
         hj[j] = HostJob{in.cube, in.num_points, in.uu, in.vv, in.ww, in.vis,
                         in.weight, in.cell_size_rad, in.w_scale,
-                        in.grid_size, in.grid, in.d_num_skipped, in.d_norm};
+                        in.grid_size, in.grid, in.d_num_skipped, in.d_norm,
+                        in.frequency_hz};
     }
     DeviceGuard g(ws->device);
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ws->stream;
@@ -796,7 +807,7 @@ int weights_write_drop_in(size_t n, const T* uu, const T* vv,
     st = run_weights_write(ws, sizeof(T) == sizeof(double), 1, n,
                            ws->in_uu.ptr, ws->in_vv.ptr, ws->in_weight.ptr,
                            cell_size_rad, grid_size, ws->in_grid.ptr, d_skip,
-                           s);
+                           0.0, s);
     if (st) { cudaStreamSynchronize(s); cudaGetLastError(); return st; }
     B200_WCHECK(cudaStreamSynchronize(s));
     unsigned long long skipped = 0;
@@ -852,7 +863,7 @@ int weights_read_drop_in(size_t n, const T* uu, const T* vv,
     st = run_weights_read(ws, sizeof(T) == sizeof(double), n, ws->in_uu.ptr,
                           ws->in_vv.ptr, ws->in_weight.ptr, ws->in_vis.ptr,
                           cell_size_rad, grid_size, ws->in_grid.ptr, d_skip,
-                          s);
+                          0.0, s);
     if (st) { cudaStreamSynchronize(s); cudaGetLastError(); return st; }
     B200_WCHECK(cudaStreamSynchronize(s));
     unsigned long long skipped = 0;
@@ -922,16 +933,18 @@ int oskar_b200_weights_write(oskar_B200Workspace* ws, int data_is_double,
                              int ordered, size_t num_points, const void* uu,
                              const void* vv, const void* weight,
                              double cell_size_rad, int grid_size, void* grid,
-                             unsigned long long* d_num_skipped, void* stream)
+                             unsigned long long* d_num_skipped,
+                             double frequency_hz, void* stream)
 {
-    if (!ws) return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    if (!ws || !(frequency_hz >= 0.0) || !std::isfinite(frequency_hz))
+        return OSKAR_B200_ERR_INVALID_ARGUMENT;
     int st = check_weights_args(num_points, uu, vv, weight, grid_size, grid);
     if (st) return st;
     DeviceGuard g(ws->device);
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ws->stream;
     return run_weights_write(ws, data_is_double ? 1 : 0, ordered ? 1 : 0,
                              num_points, uu, vv, weight, cell_size_rad,
-                             grid_size, grid, d_num_skipped, s);
+                             grid_size, grid, d_num_skipped, frequency_hz, s);
 }
 
 int oskar_b200_weights_read(oskar_B200Workspace* ws, int data_is_double,
@@ -939,9 +952,11 @@ int oskar_b200_weights_read(oskar_B200Workspace* ws, int data_is_double,
                             const void* vv, const void* weight_in,
                             void* weight_out, double cell_size_rad,
                             int grid_size, const void* grid,
-                            unsigned long long* d_num_skipped, void* stream)
+                            unsigned long long* d_num_skipped,
+                            double frequency_hz, void* stream)
 {
-    if (!ws || (num_points && !weight_out))
+    if (!ws || (num_points && !weight_out) || !(frequency_hz >= 0.0) ||
+        !std::isfinite(frequency_hz))
         return OSKAR_B200_ERR_INVALID_ARGUMENT;
     int st = check_weights_args(num_points, uu, vv, weight_in, grid_size,
                                 grid);
@@ -950,7 +965,7 @@ int oskar_b200_weights_read(oskar_B200Workspace* ws, int data_is_double,
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ws->stream;
     return run_weights_read(ws, data_is_double ? 1 : 0, num_points, uu, vv,
                             weight_in, weight_out, cell_size_rad, grid_size,
-                            grid, d_num_skipped, s);
+                            grid, d_num_skipped, frequency_hz, s);
 }
 
 }  // extern "C"

@@ -60,6 +60,8 @@ struct JobDesc
     double w_scale;
     float grid_scale_f;           // the same rounded as float C computes it
     float w_scale_f;
+    double coord_scale = 1.0;     // uu, vv, ww multiplier (frequency / c, or 1)
+    float coord_scale_f = 1.0f;   // the same rounded to float (FP32 data)
     unsigned long long first;     // global index of the job's first point
     unsigned long long n;         // points of the job
     int grid_size;
@@ -219,6 +221,7 @@ struct HostJob
     void* grid;
     unsigned long long* d_num_skipped;
     double* d_norm;
+    double frequency_hz;          // 0: coordinates in wavelengths
 };
 
 // Grids a batch of jobs that share precision and kernel storage type, with
@@ -251,12 +254,17 @@ int run_weights_write(oskar_B200Workspace* ws, int data_is_double,
                       int ordered, size_t n, const void* uu, const void* vv,
                       const void* weight, double cell_size_rad,
                       int grid_size, void* grid,
-                      unsigned long long* d_num_skipped, cudaStream_t st);
+                      unsigned long long* d_num_skipped, double frequency_hz,
+                      cudaStream_t st);
 int run_weights_read(oskar_B200Workspace* ws, int data_is_double, size_t n,
                      const void* uu, const void* vv, const void* weight_in,
                      void* weight_out, double cell_size_rad, int grid_size,
                      const void* grid, unsigned long long* d_num_skipped,
-                     cudaStream_t st);
+                     double frequency_hz, cudaStream_t st);
+
+// Coordinate multiplier of scale_coords (utils/read_vis.c:54): frequency
+// over the speed of light, or 1 when frequency_hz is 0.
+double coord_scale_of(double frequency_hz);
 
 int selftest_bounded_wait(oskar_B200Workspace* ws, unsigned spins,
                           int* device_status);
@@ -269,5 +277,8 @@ cudaError_t launch_status_or(oskar_B200Workspace* ws,
                              unsigned long long* acc, cudaStream_t st);
 
 int status_from_cuda(cudaError_t e);
+
+// Validates an options struct for data of the given precision.
+int check_options(const oskar_B200Options* opt, int data_is_double);
 
 }  // namespace b200

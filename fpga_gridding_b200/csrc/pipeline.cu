@@ -63,6 +63,11 @@ DeviceBuffer::~DeviceBuffer() { release(); }
         if (e_ != cudaSuccess) return status_from_cuda(e_); \
     } while (0)
 
+double coord_scale_of(double frequency_hz)
+{
+    return frequency_hz > 0.0 ? frequency_hz / 299792458.0 : 1.0;
+}
+
 int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
               int num_jobs, const HostJob* jobs, cudaStream_t st)
 {
@@ -142,6 +147,8 @@ int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
         // float (oskar_grid_wproj.c:150).
         d.grid_scale_f = (float)h.grid_size * (float)h.cell_size_rad;
         d.w_scale_f = (float)h.w_scale;
+        d.coord_scale = coord_scale_of(h.frequency_hz);
+        d.coord_scale_f = (float)d.coord_scale;
         d.first = first;
         d.n = h.num_points;
         d.grid_size = h.grid_size;
@@ -329,6 +336,7 @@ int run_grid(oskar_B200Workspace* ws, const oskar_B200Cube* cube,
     j.grid = grid;
     j.d_num_skipped = d_num_skipped;
     j.d_norm = d_norm;
+    j.frequency_hz = opt->frequency_hz;
     return run_batch(ws, opt, 1, &j, st);
 }
 

@@ -128,7 +128,9 @@ prep_kernel(const PrepArgs a)
         const size_t g = first + i;
         Placed p{};
         if (in_range)
-            p = place_one<T, MODE>(uu[i], vv[i], ww[i], pc, jd.support);
+            p = place_one<T, MODE>(scale_coord(uu[i], jd),
+                                   scale_coord(vv[i], jd),
+                                   scale_coord(ww[i], jd), pc, jd.support);
         const bool keep = in_range && !p.skipped;
         if (in_range)
         {

@@ -101,6 +101,19 @@ __device__ __forceinline__ Placed place_one(T u, T v, T w,
     return p;
 }
 
+// Metres to wavelengths as scale_coords (utils/read_vis.c:51-73) does on the
+// host: one multiplication in the data's precision (the FP64 scale rounded
+// to float for FP32 data).  The scale is exactly 1 when no frequency is
+// given, and x * 1 == x.
+__device__ __forceinline__ double scale_coord(double x, const JobDesc& jd)
+{
+    return __dmul_rn(x, jd.coord_scale);
+}
+__device__ __forceinline__ float scale_coord(float x, const JobDesc& jd)
+{
+    return __fmul_rn(x, jd.coord_scale_f);
+}
+
 // Prep of a batch: launch grid (blocks_per_job, num_jobs), block (x, j)
 // walks job j's points.
 struct PrepArgs

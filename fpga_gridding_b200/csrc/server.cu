@@ -11,6 +11,7 @@
 // arrive while others are on the device start as soon as a slot and memory
 // are free.  Completion is detected by polling a CUDA event per slot; the
 // job's skip count, norm and status are copied back through pinned memory.
+#include <cmath>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -236,7 +237,8 @@ struct oskar_B200Server
                                   p.req.vv, p.req.ww, p.req.vis, p.req.weight,
                                   p.req.cell_size_rad, p.req.w_scale,
                                   p.req.grid_size, g, outs,
-                                  reinterpret_cast<double*>(outs + 1)};
+                                  reinterpret_cast<double*>(outs + 1),
+                                  p.req.frequency_hz};
             }
             if (!ok && s.jobs.empty()) break;
             jobs.resize(s.jobs.size());
@@ -371,7 +373,8 @@ int oskar_b200_server_submit(oskar_B200Server* s, const oskar_B200Request* r)
     if (!s || !r || !r->cube || r->cube->device != s->device ||
         r->grid_size < 1 || r->grid_size > 65535 ||
         (r->num_points && (!r->uu || !r->vv || !r->ww || !r->vis)) ||
-        (s->opt.apply_weight && r->num_points && !r->weight))
+        (s->opt.apply_weight && r->num_points && !r->weight) ||
+        !(r->frequency_hz >= 0.0) || !std::isfinite(r->frequency_hz))
         return OSKAR_B200_ERR_INVALID_ARGUMENT;
     Pending p;
     p.req = *r;

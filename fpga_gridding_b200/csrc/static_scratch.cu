@@ -178,6 +178,8 @@ extern "C" int oskar_b200_grid_f_static(
     jd.w_scale = w_scale;
     jd.grid_scale_f = (float)grid_size * cell_size_rad;
     jd.w_scale_f = w_scale;
+    jd.coord_scale = 1.0;       // coordinates are in wavelengths
+    jd.coord_scale_f = 1.0f;
     jd.first = 0;
     jd.n = n;
     jd.grid_size = grid_size;

@@ -4,6 +4,8 @@
 // Both steps place a point at the cell
 //   grid_u = (int)round(-u * grid_size * cell) + grid_size / 2,
 //   grid_v = (int)round( v * grid_size * cell) + grid_size / 2
+// (u, v first scaled from metres to wavelengths as scale_coords does, when a
+// frequency is given)
 // and skip it when the cell is outside the grid.  The weights grid is real
 // (one value per cell), row-major in v.
 //
@@ -30,6 +32,8 @@ struct WeightConsts
 {
     double grid_scale;   // grid_size * cell_size_rad, FP64
     float grid_scale_f;  // the same product in float arithmetic
+    double coord_scale;  // metres to wavelengths (scale_coords), or 1
+    float coord_scale_f;
     int grid_size;
     int centre;
 };
@@ -44,8 +48,10 @@ __device__ __forceinline__ long long weight_cell(T u, T v,
     long long gu, gv;
     if (sizeof(T) == sizeof(double))
     {
-        const double ru = round(__dmul_rn(-(double)u, c.grid_scale));
-        const double rv = round(__dmul_rn((double)v, c.grid_scale));
+        const double us = __dmul_rn((double)u, c.coord_scale);
+        const double vs = __dmul_rn((double)v, c.coord_scale);
+        const double ru = round(__dmul_rn(-us, c.grid_scale));
+        const double rv = round(__dmul_rn(vs, c.grid_scale));
         gu = (ru > -2147483649.0 && ru < 2147483648.0 ? (long long)ru
                                                         : (long long)INT_MIN);
         gv = (rv > -2147483649.0 && rv < 2147483648.0 ? (long long)rv
@@ -53,8 +59,10 @@ __device__ __forceinline__ long long weight_cell(T u, T v,
     }
     else
     {
-        const float ru = roundf(__fmul_rn(-(float)u, c.grid_scale_f));
-        const float rv = roundf(__fmul_rn((float)v, c.grid_scale_f));
+        const float us = __fmul_rn((float)u, c.coord_scale_f);
+        const float vs = __fmul_rn((float)v, c.coord_scale_f);
+        const float ru = roundf(__fmul_rn(-us, c.grid_scale_f));
+        const float rv = roundf(__fmul_rn(vs, c.grid_scale_f));
         gu = (ru > -2147483649.0f && ru < 2147483648.0f ? (long long)ru
                                                           : (long long)INT_MIN);
         gv = (rv > -2147483649.0f && rv < 2147483648.0f ? (long long)rv
@@ -249,12 +257,14 @@ weights_read_kernel(size_t n, const T* __restrict__ uu,
 }
 
 WeightConsts make_consts(int data_is_double, double cell_size_rad,
-                         int grid_size)
+                         int grid_size, double frequency_hz)
 {
     WeightConsts c;
     c.grid_scale = grid_size * cell_size_rad;
     // C evaluates int * float in float (FLT_EVAL_METHOD 0 on x86-64).
     c.grid_scale_f = (float)grid_size * (float)cell_size_rad;
+    c.coord_scale = coord_scale_of(frequency_hz);
+    c.coord_scale_f = (float)c.coord_scale;
     (void)data_is_double;
     c.grid_size = grid_size;
     c.centre = grid_size / 2;
@@ -294,7 +304,8 @@ int run_weights_write(oskar_B200Workspace* ws, int data_is_double,
                       int ordered, size_t n, const void* uu, const void* vv,
                       const void* weight, double cell_size_rad,
                       int grid_size, void* grid,
-                      unsigned long long* d_num_skipped, cudaStream_t st)
+                      unsigned long long* d_num_skipped, double frequency_hz,
+                      cudaStream_t st)
 {
     B200_TRY(ws->counters.ensure(sizeof(unsigned long long) * CNT_COUNT));
     unsigned long long* skipped = skip_counter(ws, d_num_skipped);
@@ -306,7 +317,7 @@ int run_weights_write(oskar_B200Workspace* ws, int data_is_double,
         return OSKAR_B200_OK;
     }
     const WeightConsts c = make_consts(data_is_double, cell_size_rad,
-                                       grid_size);
+                                       grid_size, frequency_hz);
     const int blocks = launch_blocks(ws, n);
     if (!ordered)
     {
@@ -365,7 +376,7 @@ int run_weights_read(oskar_B200Workspace* ws, int data_is_double, size_t n,
                      const void* uu, const void* vv, const void* weight_in,
                      void* weight_out, double cell_size_rad, int grid_size,
                      const void* grid, unsigned long long* d_num_skipped,
-                     cudaStream_t st)
+                     double frequency_hz, cudaStream_t st)
 {
     B200_TRY(ws->counters.ensure(sizeof(unsigned long long) * CNT_COUNT));
     unsigned long long* skipped = skip_counter(ws, d_num_skipped);
@@ -373,7 +384,7 @@ int run_weights_read(oskar_B200Workspace* ws, int data_is_double, size_t n,
     ws->last_launches = 0;
     if (n == 0) return OSKAR_B200_OK;
     const WeightConsts c = make_consts(data_is_double, cell_size_rad,
-                                       grid_size);
+                                       grid_size, frequency_hz);
     const int blocks = launch_blocks(ws, n);
     if (data_is_double)
         weights_read_kernel<double><<<blocks, 256, 0, st>>>(

@@ -282,6 +282,7 @@ def grid_batch_device(ws: Workspace, jobs, opts: Options | None = None,
         arr[i].cell_size_rad = float(j["cell_size_rad"])
         arr[i].w_scale = float(j["w_scale"])
         arr[i].grid_size = int(j["grid_size"])
+        arr[i].frequency_hz = float(j.get("frequency_hz", 0.0))
     check(lib.oskar_b200_grid_batch(ws.handle, C.byref(opts), len(jobs), arr,
                                     _stream_ptr(stream)),
           "oskar_b200_grid_batch")
@@ -310,24 +311,77 @@ def place_device(ws: Workspace, support, oversample: int, uu, vv, ww,
 
 def weights_write_device(ws: Workspace, uu, vv, weight, cell_size_rad,
                          grid_size: int, grid, num_skipped=None,
-                         ordered: bool = True, stream=None):
+                         ordered: bool = True, frequency_hz: float = 0.0,
+                         stream=None):
     """Weights-grid histogram on torch CUDA tensors (float32 or float64);
     grid (grid_size^2 reals) accumulates.  ordered=True is bit-identical to
-    the reference; ordered=False uses one atomic add per point."""
+    the reference; ordered=False uses one atomic add per point.
+    frequency_hz > 0: uu, vv are in metres (scaled as scale_coords does)."""
     dbl = uu.dtype.is_floating_point and uu.element_size() == 8
     check(ws._lib.oskar_b200_weights_write(
         ws.handle, int(dbl), int(ordered), uu.numel(), _ptr(uu), _ptr(vv),
         _ptr(weight), float(cell_size_rad), grid_size, _ptr(grid),
-        _ptr(num_skipped), _stream_ptr(stream)), "weights_write")
+        _ptr(num_skipped), float(frequency_hz), _stream_ptr(stream)),
+        "weights_write")
 
 
 def weights_read_device(ws: Workspace, uu, vv, weight_in, weight_out,
                         cell_size_rad, grid_size: int, grid,
-                        num_skipped=None, stream=None):
+                        num_skipped=None, frequency_hz: float = 0.0,
+                        stream=None):
     """Density lookup on torch CUDA tensors: weight_out = weight_in /
     grid[cell] (0 for empty cells; skipped points keep weight_out)."""
     dbl = uu.element_size() == 8
     check(ws._lib.oskar_b200_weights_read(
         ws.handle, int(dbl), uu.numel(), _ptr(uu), _ptr(vv), _ptr(weight_in),
         _ptr(weight_out), float(cell_size_rad), grid_size, _ptr(grid),
-        _ptr(num_skipped), _stream_ptr(stream)), "weights_read")
+        _ptr(num_skipped), float(frequency_hz), _stream_ptr(stream)),
+        "weights_read")
+
+
+class Blocks:
+    """Block ingest (oskar_b200_blocks_*): host visibility blocks streamed
+    into one device grid.  push() takes host numpy arrays (the cube's
+    precision) and returns once they have been copied; the block grids
+    while the caller prepares the next.  finish() waits and returns the
+    total number of skipped points."""
+
+    def __init__(self, ws: Workspace, cube: Cube, cell_size_rad: float,
+                 w_scale: float, grid_size: int, grid, d_norm=None,
+                 opts: Options | None = None):
+        self._lib = load()
+        self._keep = (ws, cube, grid, d_norm)
+        self.handle = C.c_void_p()
+        check(self._lib.oskar_b200_blocks_create(
+            ws.handle, cube.handle, C.byref(opts) if opts is not None else None,
+            float(cell_size_rad), float(w_scale), grid_size, _ptr(grid),
+            _ptr(d_norm), C.byref(self.handle)), "blocks_create")
+        self._real = np.float64 if cube.data_is_double else np.float32
+
+    def push(self, uu, vv, ww, vis, weight=None, frequency_hz: float = 0.0):
+        r = self._real
+        arrs = [np.ascontiguousarray(a, dtype=r) for a in (uu, vv, ww, vis)]
+        w = np.ascontiguousarray(weight, dtype=r) if weight is not None \
+            else None
+        check(self._lib.oskar_b200_blocks_push(
+            self.handle, arrs[0].size, *[a.ctypes.data_as(C.c_void_p)
+                                         for a in arrs],
+            w.ctypes.data_as(C.c_void_p) if w is not None else None,
+            float(frequency_hz)), "blocks_push")
+
+    def finish(self) -> int:
+        sk = C.c_ulonglong(0)
+        check(self._lib.oskar_b200_blocks_finish(self.handle, C.byref(sk)),
+              "blocks_finish")
+        return sk.value
+
+    def close(self):
+        if self.handle:
+            self._lib.oskar_b200_blocks_free(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

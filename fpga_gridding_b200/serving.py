@@ -42,7 +42,8 @@ class Server:
         self._meta = {}       # tag -> (grid_size, dtype)
 
     def submit(self, tag: int, cube, uu, vv, ww, vis, weight,
-               cell_size_rad: float, w_scale: float, grid_size: int) -> None:
+               cell_size_rad: float, w_scale: float, grid_size: int,
+               frequency_hz: float = 0.0) -> None:
         r = Request()
         r.tag = tag
         r.cube = cube.handle
@@ -52,6 +53,7 @@ class Server:
         r.cell_size_rad = float(cell_size_rad)
         r.w_scale = float(w_scale)
         r.grid_size = int(grid_size)
+        r.frequency_hz = float(frequency_hz)
         self._inflight[tag] = (uu, vv, ww, vis, weight, cube)
         self._meta[tag] = (grid_size, uu.dtype)
         check(self._lib.oskar_b200_server_submit(self.handle, C.byref(r)),

@@ -187,7 +187,13 @@ typedef struct oskar_B200Options
                             * footprint centre lies within this many cells of
                             * the grid centre (the heavily hit cells);
                             * 0: everywhere */
-    int reserved[9];
+    int reserved0;
+    double frequency_hz; /* > 0: uu, vv, ww are in metres; they are scaled to
+                          * wavelengths by frequency_hz / c in the data's
+                          * precision before placement, exactly as
+                          * scale_coords (utils/read_vis.c:51-73) does on the
+                          * host; 0: they are in wavelengths already */
+    int reserved[6];
 } oskar_B200Options;
 
 /* Fills the defaults (FP64 coordinates, native kernels, plain accumulation,
@@ -252,6 +258,7 @@ typedef struct oskar_B200Job
     void* grid;
     unsigned long long* d_num_skipped;
     double* d_norm;
+    double frequency_hz;   /* as oskar_B200Options::frequency_hz, per job */
 } oskar_B200Job;
 
 /* Grids many independent jobs (channels, snapshots) with uneven sizes and
@@ -280,7 +287,8 @@ OSKAR_B200_EXPORT int oskar_b200_place(oskar_B200Workspace* ws,
 /* Uniform weighting on device arrays (FP64 when data_is_double, else FP32
  * with the reference's float coordinate arithmetic), asynchronous on
  * `stream`.  *d_num_skipped (device, may be NULL) is reset, then counts the
- * points outside the grid.
+ * points outside the grid.  frequency_hz > 0: uu, vv are in metres and are
+ * scaled as scale_coords does first (see oskar_B200Options).
  * write: grid (device, grid_size^2 reals) accumulates the weights.
  *   ordered = 1 adds each cell's weights in point order, bit-identical to
  *   oskar_grid_weights_write_{d,f} (stable sort by cell, then one
@@ -293,12 +301,35 @@ OSKAR_B200_EXPORT int oskar_b200_weights_write(oskar_B200Workspace* ws,
         int data_is_double, int ordered, size_t num_points, const void* uu,
         const void* vv, const void* weight, double cell_size_rad,
         int grid_size, void* grid, unsigned long long* d_num_skipped,
-        void* stream);
+        double frequency_hz, void* stream);
 OSKAR_B200_EXPORT int oskar_b200_weights_read(oskar_B200Workspace* ws,
         int data_is_double, size_t num_points, const void* uu, const void* vv,
         const void* weight_in, void* weight_out, double cell_size_rad,
         int grid_size, const void* grid, unsigned long long* d_num_skipped,
-        void* stream);
+        double frequency_hz, void* stream);
+
+/* Block ingest: visibility blocks in host memory (pageable or pinned), as
+ * the reference's main loop reads them (main.cpp:413-535), gridded into one
+ * device grid.  Each pushed block is copied to the device on a copy stream
+ * and gridded on the workspace's stream when its copy lands, with the
+ * metres-to-wavelengths scaling of scale_coords (utils/read_vis.c:51-73)
+ * done in the prep kernel when frequency_hz > 0.  push() returns once the
+ * block's data has been copied (the caller may then refill its buffers)
+ * while the block grids; the next push uploads while it grids.  `grid` and
+ * `d_norm` (device, d_norm may be NULL) accumulate.  The workspace is busy
+ * until finish(), which waits for every block and returns the total skip
+ * count.  Options as oskar_b200_grid (frequency_hz there is ignored). */
+typedef struct oskar_B200Blocks oskar_B200Blocks;
+OSKAR_B200_EXPORT int oskar_b200_blocks_create(oskar_B200Workspace* ws,
+        const oskar_B200Cube* cube, const oskar_B200Options* opt,
+        double cell_size_rad, double w_scale, int grid_size, void* grid,
+        double* d_norm, oskar_B200Blocks** blocks);
+OSKAR_B200_EXPORT int oskar_b200_blocks_push(oskar_B200Blocks* blocks,
+        size_t num_points, const void* uu, const void* vv, const void* ww,
+        const void* vis, const void* weight, double frequency_hz);
+OSKAR_B200_EXPORT int oskar_b200_blocks_finish(oskar_B200Blocks* blocks,
+        unsigned long long* num_skipped);
+OSKAR_B200_EXPORT int oskar_b200_blocks_free(oskar_B200Blocks* blocks);
 
 /* Statistics of the most recent oskar_b200_grid call on this workspace
  * (valid once its stream has been synchronised). */
@@ -392,6 +423,7 @@ typedef struct oskar_B200Request
     double cell_size_rad;
     double w_scale;
     int grid_size;
+    double frequency_hz;           /* as oskar_B200Options::frequency_hz */
 } oskar_B200Request;
 
 typedef struct oskar_B200Completion

@@ -950,3 +950,36 @@ double orc_time_weights_parallel_f(orc_wwrite_fn_f wfn, orc_wread_fn_f rfn,
     free(grids);
     return worst;
 }
+
+/* ------------------------------------------------------------------ */
+/* Coordinate scaling (utils/read_vis.c:51-73).                         */
+/* ------------------------------------------------------------------ */
+
+void orc_scale_coords(double freq_hz, int is_double, size_t num_coords,
+        void* uu, void* vv, void* ww)
+{
+    size_t i;
+    /* metres to wavelengths: times frequency over the speed of light */
+    const double s = freq_hz / 299792458.0;
+    if (is_double)
+    {
+        double* u = (double*)uu; double* v = (double*)vv; double* w = (double*)ww;
+        for (i = 0; i < num_coords; ++i)
+        {
+            u[i] = u[i] * s;
+            v[i] = v[i] * s;
+            w[i] = w[i] * s;
+        }
+    }
+    else
+    {
+        const float sf = (float)s;
+        float* u = (float*)uu; float* v = (float*)vv; float* w = (float*)ww;
+        for (i = 0; i < num_coords; ++i)
+        {
+            u[i] = u[i] * sf;
+            v[i] = v[i] * sf;
+            w[i] = w[i] * sf;
+        }
+    }
+}

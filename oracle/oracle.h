@@ -96,6 +96,12 @@ void orc_grid_weights_read_f(size_t num_points, const float* uu,
         float cell_size_rad, int grid_size, size_t* num_skipped,
         const float* grid);
 
+/* Coordinates in metres to wavelengths, restating utils/read_vis.c:51-73:
+ * every coordinate times freq_hz / c, in the data's precision (the double
+ * scale is rounded to float for FP32 data).  is_double selects the type. */
+void orc_scale_coords(double freq_hz, int is_double, size_t num_coords,
+        void* uu, void* vv, void* ww);
+
 /* ------------------------------------------------------------------------
  * CPU baseline harness.  Runs a gridding function (the compiled reference's
  * or this restatement's, passed as a pointer) on num_threads threads, each

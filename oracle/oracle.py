@@ -8,6 +8,9 @@ bench.py's CPU-baseline leg import this module.  It wraps:
                            oskar_grid_weights.c compiled unmodified
                            (present where the reference sources were
                            available at build time).
+  _ref/libref_ingest.so    the reference's read_vis.c (read_coords,
+                           scale_coords) and OSKAR binary file library,
+                           compiled unmodified (same condition).
 
 Build both with `make -C oracle`.
 """
@@ -22,6 +25,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libref_gridder.so")
+REF_INGEST_SO = os.path.join(HERE, "_ref", "libref_ingest.so")
 
 _P = C.c_void_p
 _SZ = C.c_size_t
@@ -86,6 +90,8 @@ def oracle_lib():
             _P, _P, C.c_int, _SZ, _P, _P, _P, C.c_float, C.c_int, _P, _P,
             _P, _P]
         lib.orc_time_weights_parallel_f.restype = C.c_double
+        lib.orc_scale_coords.argtypes = [C.c_double, C.c_int, _SZ, _P, _P, _P]
+        lib.orc_scale_coords.restype = None
         _oracle = lib
     return _oracle
 
@@ -105,6 +111,43 @@ def reference_lib():
             w.restype = r.restype = None
         _ref = lib
     return _ref
+
+
+_ref_ingest = None
+
+
+def reference_ingest_lib():
+    """The reference's read_vis.c + OSKAR binary library, or None."""
+    global _ref_ingest
+    if _ref_ingest is None:
+        if not os.path.exists(REF_INGEST_SO):
+            return None
+        lib = C.CDLL(REF_INGEST_SO)
+        lib.ref_scale_coords.argtypes = [C.c_double, C.c_int, _SZ, _P, _P, _P]
+        lib.ref_scale_coords.restype = None
+        _ref_ingest = lib
+    return _ref_ingest
+
+
+def scale_coords(freq_hz: float, uu, vv, ww, use_reference: bool = False):
+    """Metres to wavelengths as utils/read_vis.c:51-73 (restated, or the
+    reference's own function): returns scaled copies in the arrays'
+    precision (float32 or float64)."""
+    a = [np.array(x, copy=True) for x in (uu, vv, ww)]
+    dbl = a[0].dtype == np.float64
+    assert all(x.dtype == a[0].dtype and x.flags.c_contiguous for x in a)
+    if use_reference:
+        lib = reference_ingest_lib()
+        if lib is None:
+            raise RuntimeError("reference ingest library not built")
+        # OSKAR_DOUBLE = 0x08, OSKAR_SINGLE = 0x04
+        # (utils/binary/oskar_binary_data_types.h:52-55)
+        lib.ref_scale_coords(freq_hz, 0x08 if dbl else 0x04, a[0].size,
+                             _ptr(a[0]), _ptr(a[1]), _ptr(a[2]))
+    else:
+        oracle_lib().orc_scale_coords(freq_hz, int(dbl), a[0].size,
+                                      _ptr(a[0]), _ptr(a[1]), _ptr(a[2]))
+    return a
 
 
 def _ptr(a):

@@ -186,6 +186,20 @@ def test_weights_parallel_harness_matches_serial_for_unit_weights(oracle,
         assert np.array_equal(grid, g1) and np.array_equal(wout, w1)
 
 
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_scale_coords_restatement_matches_reference(oracle, ref, dtype):
+    if oracle.reference_ingest_lib() is None:
+        pytest.skip("reference ingest library not built")
+    rng = np.random.default_rng(8)
+    uu, vv, ww = (rng.normal(0.0, 3000.0, 50000).astype(dtype)
+                  for _ in range(3))
+    for f in (50e6, 149.97e6, 1.4204e9):
+        a = oracle.scale_coords(f, uu, vv, ww)
+        b = oracle.scale_coords(f, uu, vv, ww, use_reference=True)
+        for x, y in zip(a, b):
+            assert x.dtype == dtype and np.array_equal(x, y)
+
+
 def test_parallel_timing_harness_sums_to_serial(oracle, small):
     secs, sk, nrm, grid = oracle.time_parallel(small, False, 3, False,
                                                want_grid=True)
