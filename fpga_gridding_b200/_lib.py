@@ -25,6 +25,7 @@ EXPORTED_SYMBOLS = (
     "oskar_b200_workspace_free",
     "oskar_b200_workspace_bytes",
     "oskar_b200_cube_create",
+    "oskar_b200_cube_create_planar",
     "oskar_b200_cube_free",
     "oskar_b200_cube_bytes",
     "oskar_b200_grid",
@@ -168,6 +169,9 @@ def load():
     lib.oskar_b200_workspace_bytes.restype = _SZ
     lib.oskar_b200_cube_create.argtypes = [
         _P, _SZ, _P, C.c_int, C.c_int, _P, C.c_int, C.c_int, C.c_int,
+        C.c_int, _P, C.POINTER(_P)]
+    lib.oskar_b200_cube_create_planar.argtypes = [
+        _P, _SZ, _P, C.c_int, C.c_int, _P, _P, C.c_int, C.c_int, C.c_int,
         C.c_int, _P, C.POINTER(_P)]
     lib.oskar_b200_cube_free.argtypes = [_P]
     lib.oskar_b200_cube_bytes.argtypes = [_P]

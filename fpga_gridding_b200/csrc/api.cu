@@ -165,8 +165,8 @@ int validate_cube_args(size_t num_w_planes, const int* support,
 // Builds (or rebuilds) `cube` in place from a device copy of the cube.
 int cube_init(oskar_B200Cube* c, int device, size_t num_w_planes,
               const int* support, int oversample, int conv_size_half,
-              const void* d_conv, int conv_is_double, int data_is_double,
-              int kernel_type, cudaStream_t st)
+              const void* d_conv, const void* d_conv_im, int conv_is_double,
+              int data_is_double, int kernel_type, cudaStream_t st)
 {
     c->device = device;
     c->num_planes = (int)num_w_planes;
@@ -192,7 +192,7 @@ int cube_init(oskar_B200Cube* c, int device, size_t num_w_planes,
                             sizeof(int) * num_w_planes,
                             cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return status_from_cuda(e);
-    return cube_build(c, d_conv, conv_is_double, st);
+    return cube_build(c, d_conv, d_conv_im, conv_is_double, st);
 }
 
 
@@ -297,7 +297,7 @@ int drop_in(size_t num_w_planes, const int* support, int oversample,
     B200_CHECK(cudaEventRecord(ev_cube, c));
     B200_CHECK(cudaStreamWaitEvent(s, ev_cube, 0));
     st = cube_init(tc.cube, device, num_w_planes, support, oversample,
-                   conv_size_half, ws->in_cube.ptr, dbl, dbl,
+                   conv_size_half, ws->in_cube.ptr, nullptr, dbl, dbl,
                    OSKAR_B200_KERNEL_NATIVE, s);
     if (st) { cudaStreamSynchronize(s); cudaStreamSynchronize(c);
               cudaGetLastError(); return st; }
@@ -495,12 +495,19 @@ size_t oskar_b200_workspace_bytes(const oskar_B200Workspace* ws)
     return t;
 }
 
-int oskar_b200_cube_create(oskar_B200Workspace* ws, size_t num_w_planes,
-                           const int* support, int oversample,
-                           int conv_size_half, const void* conv_func,
-                           int conv_func_is_double, int conv_func_on_device,
-                           int data_is_double, int kernel_type, void* stream,
-                           oskar_B200Cube** cube)
+}  // extern "C"
+
+namespace {
+
+// Shared body of the cube constructors: conv_im == nullptr means conv_func is
+// the interleaved complex cube; otherwise conv_func / conv_im are the real /
+// imaginary parts.
+int cube_create_impl(oskar_B200Workspace* ws, size_t num_w_planes,
+                     const int* support, int oversample, int conv_size_half,
+                     const void* conv_func, const void* conv_im,
+                     int conv_func_is_double, int conv_func_on_device,
+                     int data_is_double, int kernel_type, void* stream,
+                     oskar_B200Cube** cube)
 {
     if (!ws || !cube) return OSKAR_B200_ERR_INVALID_ARGUMENT;
     *cube = nullptr;
@@ -516,29 +523,71 @@ int oskar_b200_cube_create(oskar_B200Workspace* ws, size_t num_w_planes,
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ws->stream;
     auto* c = new (std::nothrow) oskar_B200Cube();
     if (!c) return OSKAR_B200_ERR_OUT_OF_MEMORY;
+    const size_t parts = conv_im ? 1 : 2;
     const size_t bytes = num_w_planes * (size_t)conv_size_half *
-                         conv_size_half * 2 *
+                         conv_size_half * parts *
                          (conv_func_is_double ? sizeof(double) : sizeof(float));
     const void* d_conv = conv_func;
-    DeviceBuffer staging;
+    const void* d_im = conv_im;
+    DeviceBuffer staging, staging_im;
     if (!conv_func_on_device)
     {
         cudaError_t e = staging.ensure(bytes);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(staging.ptr, conv_func, bytes,
                                 cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess && conv_im)
+        {
+            e = staging_im.ensure(bytes);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(staging_im.ptr, conv_im, bytes,
+                                    cudaMemcpyHostToDevice, s);
+        }
         if (e != cudaSuccess) { delete c; return status_from_cuda(e); }
         d_conv = staging.ptr;
+        d_im = conv_im ? staging_im.ptr : nullptr;
     }
     st = cube_init(c, ws->device, num_w_planes, support, oversample,
-                   conv_size_half, d_conv, conv_func_is_double,
+                   conv_size_half, d_conv, d_im, conv_func_is_double,
                    data_is_double, kernel_type, s);
-    // The staging copy must outlive the kernels that read it.
+    // The staging copies must outlive the kernels that read them.
     cudaError_t e = cudaStreamSynchronize(s);
     if (!st && e != cudaSuccess) st = status_from_cuda(e);
     if (st) { delete c; return st; }
     *cube = c;
     return OSKAR_B200_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int oskar_b200_cube_create(oskar_B200Workspace* ws, size_t num_w_planes,
+                           const int* support, int oversample,
+                           int conv_size_half, const void* conv_func,
+                           int conv_func_is_double, int conv_func_on_device,
+                           int data_is_double, int kernel_type, void* stream,
+                           oskar_B200Cube** cube)
+{
+    return cube_create_impl(ws, num_w_planes, support, oversample,
+                            conv_size_half, conv_func, nullptr,
+                            conv_func_is_double, conv_func_on_device,
+                            data_is_double, kernel_type, stream, cube);
+}
+
+int oskar_b200_cube_create_planar(oskar_B200Workspace* ws,
+                                  size_t num_w_planes, const int* support,
+                                  int oversample, int conv_size_half,
+                                  const void* conv_re, const void* conv_im,
+                                  int conv_is_double, int conv_on_device,
+                                  int data_is_double, int kernel_type,
+                                  void* stream, oskar_B200Cube** cube)
+{
+    if (!conv_im) return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    return cube_create_impl(ws, num_w_planes, support, oversample,
+                            conv_size_half, conv_re, conv_im, conv_is_double,
+                            conv_on_device, data_is_double, kernel_type,
+                            stream, cube);
 }
 
 int oskar_b200_cube_free(oskar_B200Cube* cube)

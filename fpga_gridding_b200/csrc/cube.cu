@@ -41,11 +41,50 @@ template <> struct Store<__nv_bfloat162>
     }
 };
 
+// The reference's cube as the kernels read it: the real and imaginary part
+// of flat element f (plane * csh^2 + row * csh + column) at re[f * stride]
+// and im[f * stride].  Interleaved (the reference's complex array,
+// main.cpp:197-201): im = re + 1, stride 2.  Planar (the separate real and
+// imaginary cubes read_kernel returns, main.cpp:182-189): stride 1.
+template <typename IN>
+struct CubeSrc
+{
+    const IN* re;
+    const IN* im;
+    int stride;
+    __device__ __forceinline__ double real(long long f) const
+    {
+        return (double)re[f * stride];
+    }
+    __device__ __forceinline__ double imag(long long f) const
+    {
+        return (double)im[f * stride];
+    }
+};
+
+template <typename IN>
+CubeSrc<IN> cube_src(const void* re, const void* im)
+{
+    CubeSrc<IN> c;
+    c.re = static_cast<const IN*>(re);
+    if (im)
+    {
+        c.im = static_cast<const IN*>(im);
+        c.stride = 1;
+    }
+    else
+    {
+        c.im = c.re + 1;
+        c.stride = 2;
+    }
+    return c;
+}
+
 // Largest |re| or |im| over each plane's used quadrant [0, E)^2, following
 // the reference's flat indexing (an index past the row end reads the next
 // row, as oskar_grid_wproj.c:110-116 does).
 template <typename IN>
-__global__ void plane_maxabs_kernel(const IN* __restrict__ cube,
+__global__ void plane_maxabs_kernel(const CubeSrc<IN> cube,
                                     const PlaneDesc* __restrict__ planes,
                                     int conv_size_half, float* __restrict__ out)
 {
@@ -57,8 +96,8 @@ __global__ void plane_maxabs_kernel(const IN* __restrict__ cube,
     {
         const int xv = e / d.extent, xu = e % d.extent;
         const long long f = base + (long long)xv * conv_size_half + xu;
-        m = fmaxf(m, fmaxf(fabsf((float)cube[2 * f]),
-                           fabsf((float)cube[2 * f + 1])));
+        m = fmaxf(m, fmaxf(fabsf((float)cube.real(f)),
+                           fabsf((float)cube.imag(f))));
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1)
@@ -75,7 +114,7 @@ __global__ void plane_maxabs_kernel(const IN* __restrict__ cube,
 }
 
 template <typename IN, typename KT>
-__global__ void relayout_kernel(const IN* __restrict__ cube,
+__global__ void relayout_kernel(const CubeSrc<IN> cube,
                                 const PlaneDesc* __restrict__ planes,
                                 int oversample, int half, int conv_size_half,
                                 KT* __restrict__ slabs)
@@ -101,8 +140,8 @@ __global__ void relayout_kernel(const IN* __restrict__ cube,
         if (col < oversample * d.L && xu < d.extent)
         {
             const long long f = base + (long long)xv * conv_size_half + xu;
-            re = (double)cube[2 * f];
-            im = (double)cube[2 * f + 1];
+            re = cube.real(f);
+            im = cube.imag(f);
         }
         slabs[d.offset + e] = Store<KT>::make(re, im, inv);
     }
@@ -113,7 +152,7 @@ __global__ void relayout_kernel(const IN* __restrict__ cube,
 // reference's order (dv outer, du inner; oskar_grid_wproj.c:104-123), so a
 // per-visibility sum is bit-identical to the reference's `sum`.
 template <typename IN>
-__global__ void norm_table_kernel(const IN* __restrict__ cube,
+__global__ void norm_table_kernel(const CubeSrc<IN> cube,
                                   const PlaneDesc* __restrict__ planes,
                                   int num_planes, int oversample, int half,
                                   int conv_size_half, double* __restrict__ table)
@@ -132,26 +171,26 @@ __global__ void norm_table_kernel(const IN* __restrict__ cube,
         const long long krow = base +
             (long long)abs(ov + dv * oversample) * conv_size_half;
         for (int du = -s; du <= s; ++du)
-            acc += (double)cube[2 * (krow + abs(ou + du * oversample))];
+            acc += cube.real(krow + abs(ou + du * oversample));
     }
     table[idx] = acc;
 }
 
 template <typename IN, typename KT>
 void launch_relayout(const oskar_B200Cube* c, const void* conv,
-                     cudaStream_t st)
+                     const void* conv_im, cudaStream_t st)
 {
     dim3 grid(64, c->num_planes);
     relayout_kernel<IN, KT><<<grid, 256, 0, st>>>(
-        static_cast<const IN*>(conv),
+        cube_src<IN>(conv, conv_im),
         static_cast<const PlaneDesc*>(c->d_planes.ptr), c->oversample,
         c->half, c->conv_size_half, static_cast<KT*>(c->d_slabs.ptr));
 }
 
 }  // namespace
 
-int cube_build(oskar_B200Cube* c, const void* d_conv, int conv_is_double,
-               cudaStream_t st)
+int cube_build(oskar_B200Cube* c, const void* d_conv, const void* d_conv_im,
+               int conv_is_double, cudaStream_t st)
 {
     const int P = c->num_planes, os = c->oversample;
     // Slab geometry and offsets (host).
@@ -201,12 +240,12 @@ int cube_build(oskar_B200Cube* c, const void* d_conv, int conv_is_double,
         if (e != cudaSuccess) return status_from_cuda(e);
         if (conv_is_double)
             plane_maxabs_kernel<double><<<P, 256, 0, st>>>(
-                static_cast<const double*>(d_conv),
+                cube_src<double>(d_conv, d_conv_im),
                 static_cast<const PlaneDesc*>(c->d_planes.ptr),
                 c->conv_size_half, static_cast<float*>(d_max.ptr));
         else
             plane_maxabs_kernel<float><<<P, 256, 0, st>>>(
-                static_cast<const float*>(d_conv),
+                cube_src<float>(d_conv, d_conv_im),
                 static_cast<const PlaneDesc*>(c->d_planes.ptr),
                 c->conv_size_half, static_cast<float*>(d_max.ptr));
         std::vector<float> h_max(P);
@@ -226,12 +265,12 @@ int cube_build(oskar_B200Cube* c, const void* d_conv, int conv_is_double,
         switch (c->kernel_type)
         {
         case OSKAR_B200_KERNEL_F16:
-            launch_relayout<double, __half2>(c, d_conv, st); break;
+            launch_relayout<double, __half2>(c, d_conv, d_conv_im, st); break;
         case OSKAR_B200_KERNEL_BF16:
-            launch_relayout<double, __nv_bfloat162>(c, d_conv, st); break;
+            launch_relayout<double, __nv_bfloat162>(c, d_conv, d_conv_im, st); break;
         default:
-            if (c->data_is_double) launch_relayout<double, double2>(c, d_conv, st);
-            else launch_relayout<double, float2>(c, d_conv, st);
+            if (c->data_is_double) launch_relayout<double, double2>(c, d_conv, d_conv_im, st);
+            else launch_relayout<double, float2>(c, d_conv, d_conv_im, st);
         }
     }
     else
@@ -239,12 +278,12 @@ int cube_build(oskar_B200Cube* c, const void* d_conv, int conv_is_double,
         switch (c->kernel_type)
         {
         case OSKAR_B200_KERNEL_F16:
-            launch_relayout<float, __half2>(c, d_conv, st); break;
+            launch_relayout<float, __half2>(c, d_conv, d_conv_im, st); break;
         case OSKAR_B200_KERNEL_BF16:
-            launch_relayout<float, __nv_bfloat162>(c, d_conv, st); break;
+            launch_relayout<float, __nv_bfloat162>(c, d_conv, d_conv_im, st); break;
         default:
-            if (c->data_is_double) launch_relayout<float, double2>(c, d_conv, st);
-            else launch_relayout<float, float2>(c, d_conv, st);
+            if (c->data_is_double) launch_relayout<float, double2>(c, d_conv, d_conv_im, st);
+            else launch_relayout<float, float2>(c, d_conv, d_conv_im, st);
         }
     }
     const int span = 2 * c->half + 1;
@@ -252,12 +291,12 @@ int cube_build(oskar_B200Cube* c, const void* d_conv, int conv_is_double,
     const int blocks = (entries + 127) / 128;
     if (conv_is_double)
         norm_table_kernel<double><<<blocks, 128, 0, st>>>(
-            static_cast<const double*>(d_conv),
+            cube_src<double>(d_conv, d_conv_im),
             static_cast<const PlaneDesc*>(c->d_planes.ptr), P, os, c->half,
             c->conv_size_half, static_cast<double*>(c->d_norm_table.ptr));
     else
         norm_table_kernel<float><<<blocks, 128, 0, st>>>(
-            static_cast<const float*>(d_conv),
+            cube_src<float>(d_conv, d_conv_im),
             static_cast<const PlaneDesc*>(c->d_planes.ptr), P, os, c->half,
             c->conv_size_half, static_cast<double*>(c->d_norm_table.ptr));
     return status_from_cuda(cudaGetLastError());
@@ -303,12 +342,13 @@ int static_cube_fill(const float* d_conv, int num_planes, int oversample,
 {
     const int half = (oversample + 1) / 2;
     relayout_kernel<float, float2><<<dim3(64, num_planes), 256, 0, st>>>(
-        d_conv, d_planes, oversample, half, conv_size_half, d_slabs);
+        cube_src<float>(d_conv, nullptr), d_planes, oversample, half,
+        conv_size_half, d_slabs);
     const int span = 2 * half + 1;
     const int entries = num_planes * span * span;
     norm_table_kernel<float><<<(entries + 127) / 128, 128, 0, st>>>(
-        d_conv, d_planes, num_planes, oversample, half, conv_size_half,
-        d_norm_table);
+        cube_src<float>(d_conv, nullptr), d_planes, num_planes, oversample,
+        half, conv_size_half, d_norm_table);
     return status_from_cuda(cudaGetLastError());
 }
 

@@ -182,8 +182,11 @@ cudaError_t radix_sort_pairs(uint32_t* keys[2], uint32_t* vals[2], size_t n,
                              int* which, int* launches);
 
 // ---- cube.cu ----------------------------------------------------------------
+// d_conv_im == nullptr: d_conv_func is the interleaved complex cube;
+// otherwise d_conv_func / d_conv_im hold the real / imaginary parts.
 int cube_build(oskar_B200Cube* cube, const void* d_conv_func,
-               int conv_func_is_double, cudaStream_t st);
+               const void* d_conv_im, int conv_func_is_double,
+               cudaStream_t st);
 
 // ---- prep.cu / grid_romein.cu ---------------------------------------------
 // Sort key, most significant first:

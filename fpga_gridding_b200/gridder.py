@@ -203,26 +203,43 @@ class Cube:
 
     def __init__(self, ws: Workspace, support, oversample: int,
                  conv_size_half: int, conv_func, data_is_double: bool,
-                 kernel_type: int = _lib.KERNEL_NATIVE, stream=None):
+                 kernel_type: int = _lib.KERNEL_NATIVE, stream=None,
+                 conv_imag=None):
+        """conv_func: the interleaved complex cube (reference layout), or,
+        with conv_imag given, its real part (the two cubes read_kernel
+        returns).  numpy arrays (host) or CUDA tensors (device)."""
         import torch
         self._lib = load()
         self.support = np.ascontiguousarray(support, dtype=np.int32)
         on_device = isinstance(conv_func, torch.Tensor) and conv_func.is_cuda
-        if isinstance(conv_func, torch.Tensor):
-            conv_func = conv_func.contiguous()
-            is_double = conv_func.dtype == torch.float64
-            ptr = C.c_void_p(conv_func.data_ptr())
-        else:
-            conv_func = np.ascontiguousarray(conv_func)
-            is_double = conv_func.dtype == np.float64
-            ptr = conv_func.ctypes.data_as(C.c_void_p)
+
+        def ref(a):
+            if isinstance(a, torch.Tensor):
+                a = a.contiguous()
+                return a, a.dtype == torch.float64, C.c_void_p(a.data_ptr())
+            a = np.ascontiguousarray(a)
+            return a, a.dtype == np.float64, a.ctypes.data_as(C.c_void_p)
+        conv_func, is_double, ptr = ref(conv_func)
+        self._keep = [conv_func]
         self.handle = C.c_void_p()
-        check(self._lib.oskar_b200_cube_create(
-            ws.handle, len(self.support),
-            self.support.ctypes.data_as(C.c_void_p), oversample,
-            conv_size_half, ptr, int(is_double), int(on_device),
-            int(data_is_double), kernel_type, _stream_ptr(stream),
-            C.byref(self.handle)), "cube_create")
+        sup = self.support.ctypes.data_as(C.c_void_p)
+        if conv_imag is None:
+            check(self._lib.oskar_b200_cube_create(
+                ws.handle, len(self.support), sup, oversample,
+                conv_size_half, ptr, int(is_double), int(on_device),
+                int(data_is_double), kernel_type, _stream_ptr(stream),
+                C.byref(self.handle)), "cube_create")
+        else:
+            conv_imag, im_double, im_ptr = ref(conv_imag)
+            if im_double != is_double:
+                raise TypeError("real and imaginary cubes differ in dtype")
+            self._keep.append(conv_imag)
+            check(self._lib.oskar_b200_cube_create_planar(
+                ws.handle, len(self.support), sup, oversample,
+                conv_size_half, ptr, im_ptr, int(is_double), int(on_device),
+                int(data_is_double), kernel_type, _stream_ptr(stream),
+                C.byref(self.handle)), "cube_create_planar")
+        self._keep = None   # the constructor is synchronous
         self.data_is_double = data_is_double
         self.kernel_type = kernel_type
 

@@ -226,6 +226,16 @@ OSKAR_B200_EXPORT int oskar_b200_cube_create(oskar_B200Workspace* ws,
         int conv_size_half, const void* conv_func, int conv_func_is_double,
         int conv_func_on_device, int data_is_double, int kernel_type,
         void* stream, oskar_B200Cube** cube);
+/* The same from the separate real and imaginary cubes
+ * ([num_w_planes][conv_size_half][conv_size_half] each) that read_kernel
+ * returns for the *_KERNELS_REAL / _IMAG FITS files (utils/read_kernel.c:
+ * 36-118, main.cpp:182-189): the interleave of main.cpp:197-201 happens in
+ * the re-layout kernel instead of on the host. */
+OSKAR_B200_EXPORT int oskar_b200_cube_create_planar(oskar_B200Workspace* ws,
+        size_t num_w_planes, const int* support, int oversample,
+        int conv_size_half, const void* conv_re, const void* conv_im,
+        int conv_is_double, int conv_on_device, int data_is_double,
+        int kernel_type, void* stream, oskar_B200Cube** cube);
 OSKAR_B200_EXPORT int oskar_b200_cube_free(oskar_B200Cube* cube);
 OSKAR_B200_EXPORT size_t oskar_b200_cube_bytes(const oskar_B200Cube* cube);
 

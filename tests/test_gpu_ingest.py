@@ -170,3 +170,44 @@ def test_invalid_frequency_rejected(ws):
     assert blocks.finish() == 0
     blocks.close()
     cube.close()
+
+
+@pytest.mark.parametrize("single", [False, True])
+@pytest.mark.parametrize("kt", [_lib.KERNEL_NATIVE, _lib.KERNEL_F16])
+def test_planar_cube_equals_interleaved(ws, single, kt):
+    """The real and imaginary cubes of the two kernel FITS files, given
+    separately: the same resident cube as the interleaved one the
+    reference's main loop builds (main.cpp:197-201): equal size, the same
+    norm to the bit (the norm table reads the real parts), and grids equal
+    up to the order of the grid atomics."""
+    if single is False and kt != _lib.KERNEL_NATIVE:
+        pytest.skip("FP64 data uses native kernels")
+    w = W.plain_small().numpy()
+    real = np.float32 if single else np.float64
+    conv = np.asarray(w["conv_func"], real)
+    re, im = conv[0::2].copy(), conv[1::2].copy()
+    g = w["grid_size"]
+    tdt = torch.float32 if single else torch.float64
+    d = lambda a: torch.as_tensor(np.asarray(a, real)).cuda()
+    cell, wsc = _scalars(w, single)
+    outs = []
+    for planar in (False, True):
+        if planar:
+            cube = fg.Cube(ws, w["support"], w["oversample"],
+                           w["conv_size_half"], re, data_is_double=not single,
+                           kernel_type=kt, conv_imag=im)
+        else:
+            cube = fg.Cube(ws, w["support"], w["oversample"],
+                           w["conv_size_half"], conv,
+                           data_is_double=not single, kernel_type=kt)
+        grid = torch.zeros(2 * g * g, dtype=tdt, device="cuda")
+        norm = torch.zeros(1, dtype=torch.float64, device="cuda")
+        fg.grid_device(ws, cube, d(w["uu"]), d(w["vv"]), d(w["ww"]),
+                       d(w["vis"]), d(w["weight"]), cell, wsc, g, grid, None,
+                       norm)
+        torch.cuda.synchronize()
+        outs.append((grid.cpu().numpy(), norm.item(), cube.bytes))
+        cube.close()
+    assert outs[0][1] == outs[1][1] and outs[0][2] == outs[1][2]
+    from oracle.oracle import rel_rms
+    assert rel_rms(outs[1][0], outs[0][0]) <= (1e-6 if single else 1e-14)
