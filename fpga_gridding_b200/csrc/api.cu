@@ -630,6 +630,46 @@ int oskar_b200_grid(oskar_B200Workspace* ws, const oskar_B200Cube* cube,
                     d_norm, s);
 }
 
+int oskar_b200_degrid(oskar_B200Workspace* ws, const oskar_B200Cube* cube,
+                      const oskar_B200Options* opt, size_t num_points,
+                      const void* uu, const void* vv, const void* ww,
+                      const void* weight, double cell_size_rad,
+                      double w_scale, int grid_size, const void* grid,
+                      void* vis, unsigned long long* d_num_skipped,
+                      void* stream)
+{
+    if (!ws || !cube) return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    oskar_B200Options defaults;
+    oskar_b200_options_init(&defaults);
+    if (!opt) opt = &defaults;
+    int st = check_options(opt, cube->data_is_double);
+    if (st) return st;
+    if (opt->accum_mode != OSKAR_B200_ACCUM_PLAIN)
+        return OSKAR_B200_ERR_UNSUPPORTED;
+    st = check_grid_args(num_points, uu, vv, ww, vis, weight,
+                         opt->apply_weight, grid_size, grid);
+    if (st) return st;
+    if (cube->device != ws->device) return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    DeviceGuard g(ws->device);
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ws->stream;
+    HostJob j{};
+    j.cube = cube;
+    j.num_points = num_points;
+    j.uu = uu;
+    j.vv = vv;
+    j.ww = ww;
+    j.vis = vis;               // written
+    j.weight = weight;
+    j.cell_size_rad = cell_size_rad;
+    j.w_scale = w_scale;
+    j.grid_size = grid_size;
+    j.grid = const_cast<void*>(grid);   // read
+    j.d_num_skipped = d_num_skipped;
+    j.d_norm = nullptr;
+    j.frequency_hz = opt->frequency_hz;
+    return run_batch(ws, opt, 1, &j, s, true);
+}
+
 int oskar_b200_grid_batch(oskar_B200Workspace* ws,
                           const oskar_B200Options* opt, int num_jobs,
                           const oskar_B200Job* jobs, void* stream)

@@ -228,9 +228,19 @@ struct HostJob
 };
 
 // Grids a batch of jobs that share precision and kernel storage type, with
-// one sort and one persistent gridding launch.
+// one sort and one persistent gridding launch.  degrid: the same placement
+// and sort, then the adjoint (degrid.cu): each job's `grid` is read and its
+// `vis` written.
 int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
-              int num_jobs, const HostJob* jobs, cudaStream_t st);
+              int num_jobs, const HostJob* jobs, cudaStream_t st,
+              bool degrid = false);
+
+// ---- degrid.cu ------------------------------------------------------------
+cudaError_t launch_degrid(const uint32_t* order, const uint32_t* sorted_keys,
+                          const int4* rec, const JobDesc* jobs, int job_shift,
+                          int apply_weight, unsigned long long* counters,
+                          size_t n, int data_is_double, int kernel_type,
+                          int num_sms, cudaStream_t st);
 
 int run_grid(oskar_B200Workspace* ws, const oskar_B200Cube* cube,
              const oskar_B200Options* opt, size_t num_points, const void* uu,

@@ -69,12 +69,14 @@ double coord_scale_of(double frequency_hz)
 }
 
 int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
-              int num_jobs, const HostJob* jobs, cudaStream_t st)
+              int num_jobs, const HostJob* jobs, cudaStream_t st,
+              bool degrid)
 {
     const oskar_B200Cube* c0 = jobs[0].cube;
     const bool dbl = c0->data_is_double != 0;
     const size_t vsz = dbl ? sizeof(double) : sizeof(float);
-    const bool comp = opt->accum_mode == OSKAR_B200_ACCUM_COMPENSATED;
+    const bool comp = !degrid &&
+                      opt->accum_mode == OSKAR_B200_ACCUM_COMPENSATED;
     int launches = 0;
     ws->last_launches = 0;
     ws->events_recorded = 0;
@@ -197,11 +199,14 @@ int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
         B200_TRY(ws->vals[0].ensure(4 * n));
         B200_TRY(ws->vals[1].ensure(4 * n));
         B200_TRY(ws->rec.ensure(16 * n));
-        B200_TRY(ws->srec.ensure(16 * n));
-        B200_TRY(ws->svis.ensure(2 * vsz * n));
-        B200_TRY(ws->flags.ensure(4 * n));
-        B200_TRY(ws->task_start.ensure(4 * (n + 2)));
-        B200_TRY(ws->task_job.ensure(4 * (n + 2)));
+        if (!degrid)
+        {
+            B200_TRY(ws->srec.ensure(16 * n));
+            B200_TRY(ws->svis.ensure(2 * vsz * n));
+            B200_TRY(ws->flags.ensure(4 * n));
+            B200_TRY(ws->task_start.ensure(4 * (n + 2)));
+            B200_TRY(ws->task_job.ensure(4 * (n + 2)));
+        }
         B200_TRY(ws->scan_tmp.ensure(std::max(radix_sort_temp_bytes(n),
                                               scan_temp_bytes(n))));
     }
@@ -211,7 +216,8 @@ int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
     pa.num_jobs = num_jobs;
     pa.blocks_per_job = bpj;
     pa.max_planes = max_planes;
-    pa.apply_weight = opt->apply_weight;
+    // (the norm is not a degridding output)
+    pa.apply_weight = degrid ? 0 : opt->apply_weight;
     pa.key = kl;
     pa.rec = static_cast<int4*>(ws->rec.ptr);
     uint32_t* keys[2] = {static_cast<uint32_t*>(ws->keys[0].ptr),
@@ -257,6 +263,21 @@ int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
     B200_TRY(radix_sort_pairs(keys, vals, n, kl.total_bits + 1,
                               ws->scan_tmp.ptr, st, &which, &launches));
     B200_TRY(mark(2));
+    if (degrid)
+    {
+        B200_TRY(mark(3));
+        B200_TRY(launch_degrid(vals[which], keys[which], pa.rec, d_jobs,
+                               kl.job_shift, opt->apply_weight, counters, n,
+                               dbl, c0->kernel_type, ws->num_sms, st));
+        launches += 1;
+        B200_TRY(mark(4));
+        ws->events_recorded = timing ? 1 : 0;
+        ws->last_launches = launches;
+        B200_TRY(cudaMemcpyAsync(ws->h_counters, counters,
+                                 sizeof(unsigned long long) * CNT_COUNT,
+                                 cudaMemcpyDeviceToHost, st));
+        return OSKAR_B200_OK;
+    }
     B200_TRY(launch_permute(vals[which], keys[which], n, counters, pa.rec,
                             d_jobs, kl.job_shift, opt->apply_weight, dbl,
                             static_cast<int4*>(ws->srec.ptr), ws->svis.ptr,

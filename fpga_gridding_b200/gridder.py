@@ -277,6 +277,22 @@ def grid_device(ws: Workspace, cube: Cube, uu, vv, ww, vis, weight,
         _ptr(d_norm), _stream_ptr(stream)), "oskar_b200_grid")
 
 
+def degrid_device(ws: Workspace, cube: Cube, uu, vv, ww, weight,
+                  cell_size_rad: float, w_scale: float, grid_size: int, grid,
+                  vis, d_num_skipped=None, opts: Options | None = None,
+                  stream=None) -> None:
+    """Asynchronous degridding (the adjoint of grid_device): reads the
+    device `grid`, writes the kept visibilities' values into `vis`."""
+    lib = load()
+    if opts is None:
+        opts = options()
+    check(lib.oskar_b200_degrid(
+        ws.handle, cube.handle, C.byref(opts), uu.numel(), _ptr(uu),
+        _ptr(vv), _ptr(ww), _ptr(weight), float(cell_size_rad),
+        float(w_scale), grid_size, _ptr(grid), _ptr(vis),
+        _ptr(d_num_skipped), _stream_ptr(stream)), "oskar_b200_degrid")
+
+
 def grid_batch_device(ws: Workspace, jobs, opts: Options | None = None,
                       stream=None) -> None:
     """Asynchronous batched gridding.  `jobs` is a sequence of dicts with

@@ -283,6 +283,24 @@ OSKAR_B200_EXPORT int oskar_b200_grid_batch(oskar_B200Workspace* ws,
         const oskar_B200Options* opt, int num_jobs, const oskar_B200Job* jobs,
         void* stream);
 
+/* Degridding: the adjoint of oskar_b200_grid (no counterpart in the
+ * reference, whose Defines.h:48 only reserves a DEGRIDDING switch).  With
+ * the gridder's placement, skip test and tap kernel value
+ * Kt = conj?(K[plane][|off_v + j*os|][|off_u + k*os|]) (conjugated for
+ * w > 0), each kept visibility gets
+ *   vis[i] = sum over its (2S+1)^2 taps of grid[(gv+j)*G + gu+k] * conj(Kt)
+ * (times weight[i] with apply_weight), so that for any v and g
+ * <grid(v), g> = <v, degrid(g)>.  Device pointers; `grid` is read, `vis`
+ * (interleaved complex) written for kept visibilities, skipped ones keep
+ * their value and are counted in *d_num_skipped.  Options as
+ * oskar_b200_grid (plain accumulation only).  Asynchronous on `stream`. */
+OSKAR_B200_EXPORT int oskar_b200_degrid(oskar_B200Workspace* ws,
+        const oskar_B200Cube* cube, const oskar_B200Options* opt,
+        size_t num_points, const void* uu, const void* vv, const void* ww,
+        const void* weight, double cell_size_rad, double w_scale,
+        int grid_size, const void* grid, void* vis,
+        unsigned long long* d_num_skipped, void* stream);
+
 /* Per-visibility placement exactly as the gridder computes it (device
  * pointers, int32 outputs, any may be NULL): grid cell, clamped w-plane,
  * oversample offsets, conjugation sign (+1/-1) and skip flag (0/1). */

@@ -983,3 +983,53 @@ void orc_scale_coords(double freq_hz, int is_double, size_t num_coords,
         }
     }
 }
+
+/* ------------------------------------------------------------------ */
+/* Degridding (adjoint of the gridder; see oracle.h).                   */
+/* ------------------------------------------------------------------ */
+
+void orc_degrid_wproj_d(size_t num_w_planes, const int* support,
+        int oversample, int conv_size_half, const double* conv_func,
+        size_t num_points, const double* uu, const double* vv,
+        const double* ww, double cell_size_rad, double w_scale,
+        int grid_size, const double* grid, size_t* num_skipped,
+        double* vis_out)
+{
+    const size_t plane_elems = (size_t)conv_size_half * conv_size_half;
+    const double grid_scale = grid_size * cell_size_rad;
+    size_t n;
+    *num_skipped = 0;
+    for (n = 0; n < num_points; ++n)
+    {
+        Place p;
+        double re = 0.0, im = 0.0;
+        int dv, du;
+        place_d(num_w_planes, support, oversample, grid_scale, grid_size,
+                w_scale, uu[n], vv[n], ww[n], &p);
+        if (p.skipped) { *num_skipped += 1; continue; }
+        {
+            const double sgn = (double)p.conj;
+            const size_t plane_base = p.plane * plane_elems;
+            for (dv = -p.support; dv <= p.support; ++dv)
+            {
+                const size_t row = (size_t)(p.gv + dv) * (size_t)grid_size;
+                const size_t krow = plane_base + (size_t)abs(p.off_v +
+                        dv * oversample) * (size_t)conv_size_half;
+                for (du = -p.support; du <= p.support; ++du)
+                {
+                    const size_t ki = 2 * (krow +
+                            (size_t)abs(p.off_u + du * oversample));
+                    const size_t gi = 2 * (row + (size_t)(p.gu + du));
+                    /* tap value Kt = (k_re, sgn * k_im); add grid * conj(Kt) */
+                    const double k_re = conv_func[ki];
+                    const double k_im = conv_func[ki + 1] * sgn;
+                    const double g_re = grid[gi], g_im = grid[gi + 1];
+                    re += g_re * k_re + g_im * k_im;
+                    im += g_im * k_re - g_re * k_im;
+                }
+            }
+        }
+        vis_out[2 * n] = re;
+        vis_out[2 * n + 1] = im;
+    }
+}

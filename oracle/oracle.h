@@ -96,6 +96,22 @@ void orc_grid_weights_read_f(size_t num_points, const float* uu,
         float cell_size_rad, int grid_size, size_t* num_skipped,
         const float* grid);
 
+/* Degridding: the adjoint of oskar_grid_wproj_d.  The reference has no
+ * degridder (Defines.h:48 only reserves the switch), so this is defined
+ * here: with the gridder's placement and skip test
+ * (oskar_grid_wproj.c:70-101) and its tap kernel value
+ * Kt = conj?(K[plane][|off_v + j*os|][|off_u + k*os|]) (conjugated for
+ * w > 0, :110-122), each kept visibility becomes
+ *   vis[i] = sum over the (2S+1)^2 taps of grid[(gv+j)*G + gu+k] * conj(Kt)
+ * summed in FP64, rows j outer, columns k inner.  Skipped visibilities keep
+ * their vis_out value; num_skipped counts them. */
+void orc_degrid_wproj_d(size_t num_w_planes, const int* support,
+        int oversample, int conv_size_half, const double* conv_func,
+        size_t num_points, const double* uu, const double* vv,
+        const double* ww, double cell_size_rad, double w_scale,
+        int grid_size, const double* grid, size_t* num_skipped,
+        double* vis_out);
+
 /* Coordinates in metres to wavelengths, restating utils/read_vis.c:51-73:
  * every coordinate times freq_hz / c, in the data's precision (the double
  * scale is rounded to float for FP32 data).  is_double selects the type. */

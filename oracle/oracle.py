@@ -90,6 +90,10 @@ def oracle_lib():
             _P, _P, C.c_int, _SZ, _P, _P, _P, C.c_float, C.c_int, _P, _P,
             _P, _P]
         lib.orc_time_weights_parallel_f.restype = C.c_double
+        lib.orc_degrid_wproj_d.argtypes = [
+            _SZ, _P, C.c_int, C.c_int, _P, _SZ, _P, _P, _P, C.c_double,
+            C.c_double, C.c_int, _P, _P, _P]
+        lib.orc_degrid_wproj_d.restype = None
         lib.orc_scale_coords.argtypes = [C.c_double, C.c_int, _SZ, _P, _P, _P]
         lib.orc_scale_coords.restype = None
         _oracle = lib
@@ -332,6 +336,23 @@ def time_weights_parallel(uu, vv, weight, cell_size_rad, grid_size,
     if secs < 0:
         raise MemoryError("CPU baseline could not allocate private grids")
     return secs, sk_w.value, grid, sk_r.value, wout
+
+
+def degrid_d(w: dict, grid_arr, vis_out=None):
+    """The adjoint of the gridder (orc_degrid_wproj_d) on the arrays of `w`
+    (FP64) and a complex FP64 grid.  Returns (num_skipped, vis_out)."""
+    a = _arrays(w, np.float64)
+    n = a["uu"].shape[0]
+    out = np.zeros(2 * n) if vis_out is None else \
+        np.array(vis_out, dtype=np.float64, copy=True)
+    g = np.ascontiguousarray(grid_arr, dtype=np.float64)
+    sk = C.c_size_t(0)
+    oracle_lib().orc_degrid_wproj_d(
+        w["num_w_planes"], _ptr(a["support"]), w["oversample"],
+        w["conv_size_half"], _ptr(a["conv_func"]), n, _ptr(a["uu"]),
+        _ptr(a["vv"]), _ptr(a["ww"]), w["cell_size_rad"], w["w_scale"],
+        w["grid_size"], _ptr(g), C.byref(sk), _ptr(out))
+    return sk.value, out
 
 
 def rel_rms(test: np.ndarray, ref: np.ndarray) -> float:

@@ -200,6 +200,21 @@ def test_scale_coords_restatement_matches_reference(oracle, ref, dtype):
             assert x.dtype == dtype and np.array_equal(x, y)
 
 
+def test_degrid_oracle_is_the_adjoint_of_the_gridder(oracle, small):
+    """<G v, g> == <v, G^H g> for the oracle's gridder G and degridder G^H
+    on the plain_small job and a random complex grid."""
+    rng = np.random.default_rng(1)
+    g = small["grid_size"]
+    gr = rng.normal(size=2 * g * g)
+    sk, vis_adj = oracle.degrid_d(small, gr)
+    s1, _, gv = oracle.grid_d(small)
+    assert sk == s1
+    v = np.asarray(small["vis"], np.float64)
+    lhs = np.vdot(gr[0::2] + 1j * gr[1::2], gv[0::2] + 1j * gv[1::2])
+    rhs = np.vdot(vis_adj[0::2] + 1j * vis_adj[1::2], v[0::2] + 1j * v[1::2])
+    assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
+
+
 def test_parallel_timing_harness_sums_to_serial(oracle, small):
     secs, sk, nrm, grid = oracle.time_parallel(small, False, 3, False,
                                                want_grid=True)
