@@ -994,11 +994,187 @@ def run_reference_weights(args, world):
                     "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+DEGRID_DESC = ("degrid: the adjoint of plain_large's gridding - its "
+               "39,244,800 visibilities predicted from a seeded random "
+               "8192^2 complex64 grid with the same 256 w-planes (support "
+               "4->36, oversample 4); FP32, FP64 coordinates")
+
+
+def _degrid_cpu(O, hd, grid64, threads, m):
+    """The oracle's degridder (FP64; the reference has none) on a seeded
+    sample of m visibilities, split over `threads` host threads (ctypes
+    releases the GIL).  Returns (seconds, sample indices, vis)."""
+    from concurrent.futures import ThreadPoolExecutor
+    rng = np.random.default_rng(21)
+    idx = np.sort(rng.choice(len(hd["uu"]), size=m, replace=False))
+    sub = dict(hd)
+    for k in ("uu", "vv", "ww", "weight"):
+        sub[k] = np.asarray(hd[k][idx], np.float64)
+    sub["conv_func"] = np.asarray(hd["conv_func"], np.float64)
+    edges = np.linspace(0, m, threads + 1).astype(int)
+    parts = []
+    for a, b in zip(edges[:-1], edges[1:]):
+        p = dict(sub)
+        for k in ("uu", "vv", "ww", "weight"):
+            p[k] = sub[k][a:b]
+        p["vis"] = np.zeros(2 * (b - a))
+        parts.append(p)
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(threads) as ex:
+        res = list(ex.map(lambda p: O.degrid_d(p, grid64), parts))
+    secs = time.perf_counter() - t0
+    vis = np.concatenate([r[1] for r in res])
+    return secs, idx, vis
+
+
+def run_degrid(args, world, rank, local):
+    """Degridding (oskar_b200_degrid) at plain_large size."""
+    import fpga_gridding_b200 as fg
+    lib = fg.load()
+    wl = make_workload(rank, args.stations)
+    n = wl.num_points
+    g = wl.grid_size
+    cell = float(np.float32(wl.cell_size_rad))
+    wsc = float(np.float32(wl.w_scale))
+    ws = fg.Workspace(local)
+    cube = fg.Cube(ws, wl.support, wl.oversample, wl.conv_size_half,
+                   wl.conv_func, data_is_double=False)
+    gen = torch.Generator(device="cuda").manual_seed(17 + rank)
+    grid = torch.randn(2 * g * g, generator=gen, device="cuda")
+    vis = torch.zeros(2 * n, device="cuda")
+    skip = torch.zeros(1, dtype=torch.int64, device="cuda")
+    s = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    lib.oskar_b200_set_stage_timing(ws.handle, 1)
+
+    def step():
+        fg.degrid_device(ws, cube, wl.uu, wl.vv, wl.ww, wl.weight, cell, wsc,
+                         g, grid, vis, skip, stream=s)
+
+    for _ in range(args.warmup):
+        step()
+    s.synchronize()
+    barrier(world)
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    kern_ms, launches = [], 0
+    e0.record(s)
+    for _ in range(args.steps):
+        step()
+        s.synchronize()   # this step's stage events are now readable
+        st = ws.stats()
+        kern_ms.append(st.grid_ms)
+        launches += st.kernel_launches
+    e1.record(s)
+    e1.synchronize()
+    clk = clocks.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
+    taps = st.grid_updates
+    kernel_ms = statistics.mean(kern_ms)
+    # per visibility: 16-byte record, 4-byte order value, 4-byte key, 8-byte
+    # result; plus the grid read once and the kernel slabs
+    alg = n * (16 + 4 + 4 + 8) + g * g * 8 + cube.bytes
+    peak, peak_kind = measured_peaks()
+    achieved = alg / (kernel_ms * 1e-3) / 1e9
+    out = {"metric": "degridding throughput (visibilities predicted)",
+           "value": round(n * world / (ms * 1e-3) / 1e9, 4), "unit": UNIT,
+           "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": round(ms, 3), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": DATA_DESC,
+           "config": {"workload": DEGRID_DESC, "num_points": n,
+                      "grid_size": g,
+                      "l2": "inputs and grid (1.0 GB/step) larger than L2; "
+                            "no flush"},
+           "kernel_taps_per_s": taps / (kernel_ms * 1e-3),
+           "stage_ms": {"prep": round(st.prep_ms, 3),
+                        "sort": round(st.sort_ms, 3),
+                        "degrid": round(st.grid_ms, 3)},
+           "roofline": {"kernel": "degrid_kernel<float,float2>",
+                        "bound": "hbm", "achieved": round(achieved, 2),
+                        "peak": peak, "peak_source": peak_kind,
+                        "unit": "GB/s", "frac": round(achieved / peak, 4),
+                        "traffic": None,
+                        "algorithmic_bytes_per_launch": alg,
+                        "kernel_ms": round(kernel_ms, 3)},
+           "gpu_launches": launches, "skipped": int(skip.item()),
+           "clocks": clk}
+    if not args.no_e2e:
+        # Host buffers (pinned): coordinates and grid up, visibilities down,
+        # all inside the timed region, the C-ABI call in between.
+        h = {k: getattr(wl, k).cpu().pin_memory() for k in
+             ("uu", "vv", "ww", "weight")}
+        hg = grid.cpu().pin_memory()
+        hv = torch.empty(2 * n, dtype=torch.float32).pin_memory()
+        dev = {k: torch.empty_like(v, device="cuda") for k, v in h.items()}
+        dg = torch.empty_like(grid)
+        dv = torch.empty_like(vis)
+
+        def e2e_step():
+            with torch.cuda.stream(s):
+                for k in dev:
+                    dev[k].copy_(h[k], non_blocking=True)
+                dg.copy_(hg, non_blocking=True)
+            fg.degrid_device(ws, cube, dev["uu"], dev["vv"], dev["ww"],
+                             dev["weight"], cell, wsc, g, dg, dv, skip,
+                             stream=s)
+            with torch.cuda.stream(s):
+                hv.copy_(dv, non_blocking=True)
+        for _ in range(args.warmup):
+            e2e_step()
+        s.synchronize()
+        e0.record(s)
+        for _ in range(args.steps):
+            e2e_step()
+        e1.record(s)
+        e1.synchronize()
+        ems = max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
+        out["e2e"] = {"value": round(n * world / (ems * 1e-3) / 1e9, 4),
+                      "unit": UNIT, "h2d_bytes_per_step": n * 16 + g * g * 8,
+                      "d2h_bytes_per_step": n * 8,
+                      "ms_per_step": round(ems, 3),
+                      "path": "pinned host arrays copied in, "
+                              "oskar_b200_degrid (C ABI), visibilities "
+                              "copied out"}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        O = ensure_oracle()
+        hd = host_dict(wl)
+        g64 = grid.double().cpu().numpy()
+        t = host_threads()
+        # calibrate, then about cpu_seconds of work
+        secs, idx, _ = _degrid_cpu(O, hd, g64, t, 20000 * t)
+        m = int(min(n, max(20000 * t, 20000 * t / secs * args.cpu_seconds)))
+        secs, idx, cpu_vis = _degrid_cpu(O, hd, g64, t, m)
+        gpu_vis = vis.double().cpu().numpy().reshape(-1, 2)[idx].reshape(-1)
+        out["cpu_baseline"] = {
+            "value": round(m / secs / 1e9, 6), "unit": UNIT, "cores": t,
+            "kind": "port",
+            "sample": f"{m} seeded visibilities of the workload; the "
+                      f"oracle's FP64 degridder (the reference has none) on "
+                      f"{t} threads over slices; {secs:.2f} s"}
+        out["rel_err_vs_fp64"] = {
+            "vis_rel_rms": O.rel_rms(gpu_vis, cpu_vis),
+            "sample": f"the same {m} visibilities, FP32 GPU vs FP64 oracle "
+                      f"on the same float inputs and grid"}
+    cube.close()
+    return out
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return None
     if args.workload == "weights":
         return run_reference_weights(args, world)
+    if args.workload == "degrid":
+        return {"impl": "reference",
+                "unavailable": "the reference has no degridder (Defines.h:48 "
+                               "only reserves a DEGRIDDING switch)"}
+    if args.workload in ("batch128", "serving"):
+        return {"impl": "reference",
+                "unavailable": f"the reference has no {args.workload} path; "
+                               "its gridder is timed by the default workload"}
     O = ensure_oracle()
     use_ref = O.reference_lib() is not None
     wl = make_workload(0)
@@ -1049,7 +1225,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", choices=("plain_large", "batch128",
-                                           "serving", "weights"),
+                                           "serving", "weights", "degrid"),
                     default="plain_large",
                     help="plain_large (the benchmark job), batch128 (the "
                          "128-channel batching workload), serving (the "
@@ -1077,6 +1253,8 @@ def main():
             out = run_serving(args, world, rank, local)
         elif args.workload == "weights":
             out = run_weights(args, world, rank, local)
+        elif args.workload == "degrid":
+            out = run_degrid(args, world, rank, local)
         else:
             out = run_b200(args, world, rank, local)
         if rank == 0 and out is not None:

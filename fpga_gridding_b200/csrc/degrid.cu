@@ -8,12 +8,16 @@
 //   vis = sum over the (2S+1)^2 taps of grid[(gv+j)*G + gu+k] * conj(Kt).
 //
 // The visibilities arrive in the gridder's sort order (coarse tile, plane,
-// fine cell), so consecutive warps read neighbouring grid rows and the same
-// kernel slab rows from L1/L2.  One warp takes one visibility: its lanes
-// take footprint columns (32 at a time) and walk the footprint rows, so a
-// row's grid cells and kernel values are read as contiguous runs; the lane
-// sums are then reduced across the warp.  The result goes to the
-// visibility's own slot (the sort's values are the original indices).
+// fine cell); each CTA takes chunks of consecutive ones from a work queue,
+// so its warps read neighbouring grid rows and the same kernel slab rows
+// from L1.  A group of 16 lanes takes one visibility (2 per warp): its
+// lanes walk the footprint's taps in row-major order, 16 at a time (busy
+// whatever the support; the per-visibility set-up and reduction serve 2
+// visibilities at once), and the lane sums are reduced within the group.
+// Measured at plain_large: 16 lanes 28.5 ms, 8 lanes 30.2, 4 lanes 33.8,
+// 32 lanes 40.9.
+// The result goes to the visibility's own slot (the sort's values are the
+// original indices).
 #include "common.cuh"
 #include "internal.h"
 
@@ -24,10 +28,16 @@ template <typename GT> struct Cplx;
 template <> struct Cplx<float> { using type = float2; };
 template <> struct Cplx<double> { using type = double2; };
 
+constexpr int kDegridWarps = 8;     // warps per CTA
+constexpr int kGroup = 16;          // lanes per visibility
+constexpr int kGroups = 32 / kGroup;
+constexpr int kDegridMaxW = 255;   // footprint width for support <= 127
+constexpr int kDegridChunk = 128;  // visibilities per work-queue item
+
 // apply_weight: the adjoint of gridding weight * vis, i.e. the degridded
 // value times the visibility's weight.
 template <typename GT, typename KT>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kDegridWarps * 32)
 degrid_kernel(const uint32_t* __restrict__ order,
               const uint32_t* __restrict__ sorted_keys,
               const int4* __restrict__ rec, const JobDesc* __restrict__ jobs,
@@ -35,66 +45,130 @@ degrid_kernel(const uint32_t* __restrict__ order,
               unsigned long long* __restrict__ counters, size_t n)
 {
     using C2 = typename Cplx<GT>::type;
+    // slab column position of each footprint column, per lane group (a
+    // position is below the slab pitch, < 2^15 for oversample <= 32)
+    __shared__ short s_pos[kDegridWarps][kGroups][kDegridMaxW];
+    __shared__ unsigned long long s_chunk;
     const size_t valid = n - counters[CNT_SKIPPED];
-    const int lane = threadIdx.x & 31;
-    const size_t warp0 = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const size_t warps = ((size_t)gridDim.x * blockDim.x) >> 5;
-    for (size_t s = warp0; s < valid; s += warps)
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int group = lane / kGroup, gl = lane % kGroup;
+    short* pos = s_pos[warp][group];
+    // A CTA takes chunks of kDegridChunk consecutive sorted visibilities
+    // from a work queue: its warps work on neighbouring footprints and share
+    // grid lines and kernel rows in L1, and the uneven cost of the chunks
+    // (footprints of 81 to 5329 taps) balances across CTAs.
+    for (;;)
     {
-        const uint32_t i = order[s];
-        const JobDesc& jd = jobs[sorted_keys[s] >> job_shift];
-        const int4 r = rec[i];
-        const int plane = r.z & 0x7fffffff;
-        const GT sgn = r.z < 0 ? GT(-1) : GT(1);
-        const int half = jd.half, os = jd.oversample;
-        const int off_u = min(max((r.w & 0xffff) - half, -half), half);
-        const int off_v = min(max((r.w >> 16) - half, -half), half);
-        const PlaneDesc d = static_cast<const PlaneDesc*>(jd.planes)[plane];
-        const int S = d.support, W = 2 * S + 1, G = jd.grid_size;
-        const int u0 = r.x - S, v0 = r.y - S;
-        // The prep kernel keeps only footprints inside the grid; a record
-        // that says otherwise is reported and produces nothing.
-        if (u0 < 0 || v0 < 0 || u0 + W > G || v0 + W > G)
+        if (threadIdx.x == 0)
+            s_chunk = atomicAdd(&counters[CNT_TASK_NEXT], 1ull);
+        __syncthreads();
+        const size_t begin = (size_t)s_chunk * kDegridChunk;
+        __syncthreads();   // every thread has read s_chunk
+        if (begin >= valid) break;
+        const size_t end = min(valid, begin + (size_t)kDegridChunk);
+        // Each warp takes kGroups visibilities at a time, one per group of
+        // kGroup lanes (the loop bounds are the same for the whole warp).
+        for (size_t base = begin + (size_t)warp * kGroups; base < end;
+             base += (size_t)kDegridWarps * kGroups)
         {
-            if (lane == 0)
-                atomicOr(&counters[CNT_STATUS],
-                         (unsigned long long)DEV_ERR_GRID_INDEX);
-            continue;
-        }
-        const KT* __restrict__ slab =
-            static_cast<const KT*>(jd.slabs) + d.offset +
-            (long long)(off_v + half) * W * d.pitch;
-        const C2* __restrict__ grid = static_cast<const C2*>(jd.grid);
-        GT are = GT(0), aim = GT(0);
-        for (int k = lane; k < W; k += 32)
-        {
-            // quadrant column |off_u + (k - S) * os|, phase-major position
-            const int x = abs(off_u + (k - S) * os);
-            const int pos = (x % os) * d.L + x / os;
-            const KT* kp = slab + pos;
-            const C2* gp = grid + (size_t)v0 * G + u0 + k;
-#pragma unroll 4
-            for (int j = 0; j < W; ++j)
+            const size_t s = base + group;
+            bool active = s < end;
+            uint32_t i = 0;
+            const JobDesc* jd = nullptr;
+            int4 r = make_int4(0, 0, 0, 0);
+            if (active)
             {
-                const auto kv = KernelLoad<KT>::get(kp[(long long)j * d.pitch]);
-                const C2 g = gp[(size_t)j * G];
-                const GT kr = (GT)kv.x, ki = sgn * (GT)kv.y;
-                // grid * conj(Kt), Kt = (kr, ki)
-                are = fma(g.x, kr, fma(g.y, ki, are));
-                aim = fma(g.y, kr, fma(-g.x, ki, aim));
+                i = order[s];
+                jd = &jobs[sorted_keys[s] >> job_shift];
+                r = rec[i];
+            }
+            int S = 0, W = 0, u0 = 0, v0 = 0, off_u = 0, off_v = 0, half = 0;
+            int os = 1, G = 1;
+            PlaneDesc d{};
+            GT sgn = GT(1);
+            if (active)
+            {
+                const int plane = r.z & 0x7fffffff;
+                sgn = r.z < 0 ? GT(-1) : GT(1);
+                half = jd->half;
+                os = jd->oversample;
+                off_u = min(max((r.w & 0xffff) - half, -half), half);
+                off_v = min(max((r.w >> 16) - half, -half), half);
+                d = static_cast<const PlaneDesc*>(jd->planes)[plane];
+                S = d.support;
+                W = 2 * S + 1;
+                G = jd->grid_size;
+                u0 = r.x - S;
+                v0 = r.y - S;
+                // The prep kernel keeps only footprints inside the grid; a
+                // record that says otherwise is reported and skipped.
+                if (u0 < 0 || v0 < 0 || u0 + W > G || v0 + W > G ||
+                    W > kDegridMaxW)
+                {
+                    if (gl == 0)
+                        atomicOr(&counters[CNT_STATUS],
+                                 (unsigned long long)DEV_ERR_GRID_INDEX);
+                    active = false;
+                    W = 0;
+                }
+            }
+            __syncwarp();   // the previous visibilities are done with pos[]
+            // quadrant column |off_u + (k - S) * os|, phase-major position
+            for (int k = gl; k < W; k += kGroup)
+            {
+                const int x = abs(off_u + (k - S) * os);
+                pos[k] = (short)((x % os) * d.L + x / os);
+            }
+            __syncwarp();
+            GT are = GT(0), aim = GT(0);
+            if (active)
+            {
+                const KT* __restrict__ slab =
+                    static_cast<const KT*>(jd->slabs) + d.offset +
+                    (long long)(off_v + half) * W * d.pitch;
+                const C2* __restrict__ grid =
+                    static_cast<const C2*>(jd->grid) + (size_t)v0 * G + u0;
+                // The group's lanes walk the W * W taps in row-major order,
+                // kGroup at a time (contiguous grid reads within a row).
+                const int taps = W * W, dj = kGroup / W, dk = kGroup % W;
+                int j = gl / W, k = gl - (gl / W) * W;
+#pragma unroll 4
+                for (int t = gl; t < taps; t += kGroup)
+                {
+                    const auto kv = KernelLoad<KT>::get(
+                        slab[j * d.pitch + pos[k]]);
+                    const C2 g = grid[(size_t)j * G + k];
+                    const GT kr = (GT)kv.x, ki = sgn * (GT)kv.y;
+                    // grid * conj(Kt), Kt = (kr, ki)
+                    are = fma(g.x, kr, fma(g.y, ki, are));
+                    aim = fma(g.y, kr, fma(-g.x, ki, aim));
+                    k += dk;
+                    j += dj;
+                    if (k >= W)
+                    {
+                        k -= W;
+                        ++j;
+                    }
+                }
+            }
+#pragma unroll
+            for (int o = kGroup / 2; o > 0; o >>= 1)
+            {
+                are += __shfl_xor_sync(0xffffffffu, are, o);
+                aim += __shfl_xor_sync(0xffffffffu, aim, o);
+            }
+            if (active && gl == 0)
+            {
+                const size_t local = i - jd->first;
+                GT sc = (GT)d.scale;
+                if (apply_weight)
+                    sc *= static_cast<const GT*>(jd->weight)[local];
+                GT* out = static_cast<GT*>(const_cast<void*>(jd->vis));
+                out[2 * local] = are * sc;
+                out[2 * local + 1] = aim * sc;
             }
         }
-        are = warp_sum(are);
-        aim = warp_sum(aim);
-        if (lane == 0)
-        {
-            const size_t local = i - jd.first;
-            GT sc = (GT)d.scale;
-            if (apply_weight) sc *= static_cast<const GT*>(jd.weight)[local];
-            GT* out = static_cast<GT*>(const_cast<void*>(jd.vis));
-            out[2 * local] = are * sc;
-            out[2 * local + 1] = aim * sc;
-        }
+        __syncthreads();   // before thread 0 takes the next chunk
     }
 }
 
@@ -107,24 +181,25 @@ cudaError_t launch_degrid(const uint32_t* order, const uint32_t* sorted_keys,
                           int data_is_double, int kernel_type, int num_sms,
                           cudaStream_t st)
 {
-    const size_t want = (n * 32 + 255) / 256;
+    // up to 8 CTAs of 8 warps per SM, persistent over the work queue
+    const size_t want = (n + kDegridChunk - 1) / kDegridChunk;
     const size_t cap = (size_t)num_sms * 8;
     const unsigned blocks = (unsigned)(want < cap ? (want ? want : 1) : cap);
     if (data_is_double)
     {
         if (kernel_type != OSKAR_B200_KERNEL_NATIVE)
             return cudaErrorInvalidValue;
-        degrid_kernel<double, double2><<<blocks, 256, 0, st>>>(
+        degrid_kernel<double, double2><<<blocks, kDegridWarps * 32, 0, st>>>(
             order, sorted_keys, rec, jobs, job_shift, apply_weight, counters, n);
     }
     else if (kernel_type == OSKAR_B200_KERNEL_F16)
-        degrid_kernel<float, __half2><<<blocks, 256, 0, st>>>(
+        degrid_kernel<float, __half2><<<blocks, kDegridWarps * 32, 0, st>>>(
             order, sorted_keys, rec, jobs, job_shift, apply_weight, counters, n);
     else if (kernel_type == OSKAR_B200_KERNEL_BF16)
-        degrid_kernel<float, __nv_bfloat162><<<blocks, 256, 0, st>>>(
+        degrid_kernel<float, __nv_bfloat162><<<blocks, kDegridWarps * 32, 0, st>>>(
             order, sorted_keys, rec, jobs, job_shift, apply_weight, counters, n);
     else
-        degrid_kernel<float, float2><<<blocks, 256, 0, st>>>(
+        degrid_kernel<float, float2><<<blocks, kDegridWarps * 32, 0, st>>>(
             order, sorted_keys, rec, jobs, job_shift, apply_weight, counters, n);
     return cudaGetLastError();
 }
