@@ -102,26 +102,46 @@ __device__ __forceinline__ uint32_t spread9(uint32_t x)
     return x;
 }
 
-// Returns, for thread t < m, the sort key of the t-th visibility in
-// (row offset, Morton cell) order; its low 8 bits are the task-relative
-// index of that visibility and bits 26-31 its row offset + half.  Bitonic sort of one key
-// per thread: key = (off_v + half) << 26 | Morton(gu, gv low 9 bits) << 8 |
-// index (m <= 256, half <= 16); strides below 32 use warp shuffles, larger
-// ones go through shared memory.  All threads of the CTA must call it.
+// Layout of the in-task order key: (off_v + H) in the top `ob` bits, then
+// the Morton code of the low `mb` bits of (gu, gv), then (off_u + H) in
+// `ob` bits, then the task-relative index in the low 8 bits.  ob is the bit
+// width of 2H (H = ceil(oversample / 2)); mb (<= 9) takes what is left.
+struct TaskKey
+{
+    int ob, mb;
+    __device__ __forceinline__ explicit TaskKey(int half)
+    {
+        ob = 32 - __clz(2 * half);
+        mb = min(9, (32 - 8 - 2 * ob) / 2);
+    }
+    __device__ __forceinline__ uint32_t make(const int4 r, unsigned t) const
+    {
+        const uint32_t mask = (1u << mb) - 1u;
+        const uint32_t morton = spread9((uint32_t)r.x & mask) |
+                                (spread9((uint32_t)r.y & mask) << 1);
+        return ((uint32_t)(r.w >> 16) << (32 - ob)) | (morton << (8 + ob)) |
+               ((uint32_t)(r.w & 0xffff) << 8) | t;
+    }
+    __device__ __forceinline__ int row_offset(uint32_t key) const
+    {
+        return (int)(key >> (32 - ob));
+    }
+};
+
+// Returns, for thread t < m, the key of the t-th visibility of the task in
+// (row offset, Morton cell, column offset) order (TaskKey); its low 8 bits
+// are the task-relative index of that visibility.  Bitonic sort of one key
+// per thread (m <= 256); strides below 32 use warp shuffles, larger ones go
+// through shared memory.  All threads of the CTA must call it.
 __device__ __forceinline__ uint32_t task_order(const int4* __restrict__ srec,
                                           uint32_t begin, int m,
+                                          const TaskKey& tk,
                                           uint32_t* s_order)
 {
     static_assert(kTaskMax == kGridThreads, "one key per thread");
     const unsigned t = threadIdx.x;
     uint32_t key = 0xffffffffu;
-    if ((int)t < m)
-    {
-        const int4 r = srec[begin + t];
-        key = ((uint32_t)(r.w >> 16) << 26) |
-              ((spread9((uint32_t)r.x) | (spread9((uint32_t)r.y) << 1)) << 8) |
-              t;
-    }
+    if ((int)t < m) key = tk.make(srec[begin + t], t);
 #pragma unroll
     for (unsigned k = 2; k <= (unsigned)kGridThreads; k <<= 1)
     {
@@ -146,6 +166,18 @@ __device__ __forceinline__ uint32_t task_order(const int4* __restrict__ srec,
         }
     }
     return key;
+}
+
+// Two records that read the same kernel values into the same cells.  Their
+// contributions are vis_a * Kt + vis_b * Kt = (vis_a + vis_b) * Kt: the tap
+// coefficients (which fold in the conjugation) can simply be added.
+template <typename GT>
+__device__ __forceinline__ bool same_taps(const TapVis<GT>& a,
+                                          const TapVis<GT>& b)
+{
+    return a.origin == b.origin && a.mu == b.mu && a.mv == b.mv &&
+           a.tu == b.tu && a.cp == b.cp && a.cn == b.cn &&
+           a.rowbase == b.rowbase;
 }
 
 // Predicated complex flush: one vector reduction when `pred` holds, no
@@ -407,6 +439,8 @@ romein_grid_kernel(const GridArgs a)
     __shared__ unsigned s_task;
     __shared__ uint32_t s_order[kGridThreads];
     __shared__ int s_run_begin[kMaxOffsets], s_run_end[kMaxOffsets];
+    __shared__ unsigned char s_head[kTaskMax];
+    __shared__ int s_warp_heads[kGridThreads / 32];
 
     const V2* __restrict__ svis = static_cast<const V2*>(a.svis);
     unsigned long long* status = &a.counters[CNT_STATUS];
@@ -436,7 +470,7 @@ romein_grid_kernel(const GridArgs a)
         const unsigned task = s_task;
         if (task >= num_tasks) break;
         const uint32_t begin = a.task_start[task];
-        const int m = (int)(a.task_start[task + 1] - begin);
+        int m = (int)(a.task_start[task + 1] - begin);
         if (m <= 0 || m > kTaskMax)
         {
             if (threadIdx.x == 0)
@@ -475,22 +509,59 @@ romein_grid_kernel(const GridArgs a)
         // Order the task's visibilities by (row offset, cell): each run of
         // one row offset reads one W-row block of the plane's slab, and
         // consecutive visibilities are neighbours.
-        const uint32_t key = task_order(a.srec, begin, m, s_order);
+        const TaskKey tk(jd.half);
+        uint32_t key = task_order(a.srec, begin, m, tk, s_order);
         const int t = threadIdx.x;
+        TapVis<GT> tv;
         if (t < m)
         {
             const int src = (int)(key & 0xffu);
-            s_vis[t] = derive<GT>(a.srec[begin + src], svis[begin + src], d,
-                                  grid_size, jd.oversample, jd.half, status);
-            s_order[t] = key;
+            tv = derive<GT>(a.srec[begin + src], svis[begin + src], d,
+                            grid_size, jd.oversample, jd.half, status);
+            s_vis[t] = tv;
         }
         __syncthreads();
+        // Merge runs of records with the same taps (the same cell, plane
+        // and offsets: adjacent in this order): their coefficients add.
+        // Dense cells hold many visibilities with identical placements; at
+        // plain_large this removes a sixth of the taps.
+        const bool head = t < m && (t == 0 || !same_taps(tv, s_vis[t - 1]));
+        s_head[t] = head ? 1 : 0;
+        const unsigned ball = __ballot_sync(0xffffffffu, head);
+        if ((t & 31) == 0) s_warp_heads[t >> 5] = __popc(ball);
+        __syncthreads();
+        int pos = __popc(ball & ((1u << (t & 31)) - 1u)), merged = 0;
+#pragma unroll
+        for (int wi = 0; wi < kGridThreads / 32; ++wi)
+        {
+            pos += wi < (t >> 5) ? s_warp_heads[wi] : 0;
+            merged += s_warp_heads[wi];
+        }
+        if (head)
+        {
+            for (int q = t + 1; q < m && !s_head[q]; ++q)
+            {
+                tv.ar += s_vis[q].ar;
+                tv.ai += s_vis[q].ai;
+                tv.bi += s_vis[q].bi;
+                tv.br += s_vis[q].br;
+            }
+        }
+        __syncthreads();   // every run has been read
+        if (head)
+        {
+            s_vis[pos] = tv;
+            s_order[pos] = key;
+        }
+        __syncthreads();
+        m = merged;
         if (t < m)
         {
-            const int ov = (int)(key >> 26);
-            if (t == 0 || (int)(s_order[t - 1] >> 26) != ov)
+            key = s_order[t];
+            const int ov = tk.row_offset(key);
+            if (t == 0 || tk.row_offset(s_order[t - 1]) != ov)
                 s_run_begin[ov] = t;
-            if (t == m - 1 || (int)(s_order[t + 1] >> 26) != ov)
+            if (t == m - 1 || tk.row_offset(s_order[t + 1]) != ov)
                 s_run_end[ov] = t + 1;
         }
         __syncthreads();
