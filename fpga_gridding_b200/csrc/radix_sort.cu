@@ -6,7 +6,11 @@
 //      (counts[digit * num_tiles + tile]);
 //   2. exclusive scan of that array: the output position of the first key of
 //      each (digit, tile);
-//   3. rs_scatter: stable ranks inside the tile, scatter to the output.
+//   3. rs_scatter: stable ranks inside the tile, the tile's pairs reordered
+//      digit-major in shared memory, then written out as one contiguous run
+//      per digit (coalesced; scattering each pair straight to its bucket
+//      made every warp store touch 32 sectors: 2.70 -> 2.19 ms for the four
+//      passes over 39 M pairs).
 // Inside a tile each warp owns a contiguous run of 512 keys, read as 16
 // coalesced 32-key rows.  Equal digits in a row are ranked with
 // __match_any_sync against warp-private running counts, so the whole tile
@@ -176,14 +180,21 @@ rs_scatter_kernel(const uint32_t* __restrict__ keys_in,
                   uint32_t* __restrict__ vals_out)
 {
     __shared__ uint32_t s_count[kSortWarps][kRadix];
+    // the tile's pairs in digit-major (stable) order, then written out in
+    // contiguous runs per digit
+    __shared__ uint32_t s_keys[kSortTile], s_vals[kSortTile];
+    __shared__ uint32_t s_digit_start[kRadix];   // within the tile
+    __shared__ uint32_t s_digit_out[kRadix];     // global position
+    __shared__ uint32_t s_warp[32];
+    __shared__ uint32_t s_total;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lt_mask = (1u << lane) - 1u;
     for (int i = threadIdx.x; i < kSortWarps * kRadix; i += kSortThreads)
         (&s_count[0][0])[i] = 0;
     __syncthreads();
 
-    const size_t base = (size_t)blockIdx.x * kSortTile +
-                        (size_t)warp * (32 * kSortItems);
+    const size_t tile0 = (size_t)blockIdx.x * kSortTile;
+    const size_t base = tile0 + (size_t)warp * (32 * kSortItems);
     uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
 #pragma unroll
     for (int i = 0; i < kSortItems; ++i)
@@ -203,18 +214,24 @@ rs_scatter_kernel(const uint32_t* __restrict__ keys_in,
         rank[i] = before + __popc(peers & lt_mask);
     }
     __syncthreads();
-    // Turn the per-warp counts into output positions: warps in order, each
-    // digit starting at its scanned (digit, tile) offset.
-    for (int d = threadIdx.x; d < kRadix; d += kSortThreads)
+    // Per digit: the tile's count, the warps' starts inside it, and where
+    // the digit's run goes in the output.
+    static_assert(kRadix == kSortThreads, "one digit per thread");
     {
-        uint32_t run = offsets[(size_t)d * num_tiles + blockIdx.x];
+        const int d = threadIdx.x;
+        uint32_t total = 0;
 #pragma unroll
         for (int w = 0; w < kSortWarps; ++w)
         {
             const uint32_t c = s_count[w][d];
-            s_count[w][d] = run;
-            run += c;
+            s_count[w][d] = total;   // start of warp w inside the digit
+            total += c;
         }
+        const uint32_t start = block_exclusive_scan(total, s_warp, &s_total);
+        s_digit_start[d] = start;
+        s_digit_out[d] = offsets[(size_t)d * num_tiles + blockIdx.x];
+#pragma unroll
+        for (int w = 0; w < kSortWarps; ++w) s_count[w][d] += start;
     }
     __syncthreads();
 #pragma unroll
@@ -224,12 +241,23 @@ rs_scatter_kernel(const uint32_t* __restrict__ keys_in,
         if (p < n)
         {
             const unsigned d = (key[i] >> shift) & mask;
-            const uint32_t dst = s_count[warp][d] + rank[i];
-            keys_out[dst] = key[i];
-            vals_out[dst] = val[i];
+            const uint32_t local = s_count[warp][d] + rank[i];
+            s_keys[local] = key[i];
+            s_vals[local] = val[i];
         }
     }
+    __syncthreads();
+    const int tile_n = (int)min((size_t)kSortTile, n - tile0);
+    for (int q = threadIdx.x; q < tile_n; q += kSortThreads)
+    {
+        const uint32_t k = s_keys[q];
+        const unsigned d = (k >> shift) & mask;
+        const uint32_t dst = s_digit_out[d] + (uint32_t)q - s_digit_start[d];
+        keys_out[dst] = k;
+        vals_out[dst] = s_vals[q];
+    }
 }
+
 
 size_t scan_blocks(size_t n) { return (n + kScanTile - 1) / kScanTile; }
 
