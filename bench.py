@@ -1162,6 +1162,119 @@ def run_degrid(args, world, rank, local):
     return out
 
 
+PRECISION_DESC = ("precision: 512 stations uniform in a 5 km disk x 3000 "
+                  "samples at 150 MHz (392,448,000 visibilities concentrated "
+                  "near the uv origin); grid 4096^2; 128 w-planes, support "
+                  "4->32, oversample 8; FP32 inputs (FP64 mode: the same "
+                  "values promoted)")
+
+
+def run_precision(args, world, rank, local):
+    """The grid-precision modes on one long-integration job: speed of each
+    at full size, error of each against the FP64 GPU grid at full size and
+    against the CPU FP64 oracle on a seeded sample."""
+    import fpga_gridding_b200 as fg
+    from fpga_gridding_b200 import _lib, workloads as W
+    O = ensure_oracle()
+    num_times = 3000 if args.stations == 512 else 300
+    wl = W.precision_sweep(seed=3 + rank, device="cuda",
+                           num_stations=args.stations,
+                           num_times=num_times).to(dtype=torch.float32)
+    torch.cuda.empty_cache()
+    n, g = wl.num_points, wl.grid_size
+    cell = float(np.float32(wl.cell_size_rad))
+    wsc = float(np.float32(wl.w_scale))
+    ws = fg.Workspace(local)
+    lib = fg.load()
+    s = torch.cuda.Stream()
+    modes = [("fp32", False, _lib.KERNEL_NATIVE, _lib.ACCUM_PLAIN),
+             ("f16", False, _lib.KERNEL_F16, _lib.ACCUM_PLAIN),
+             ("bf16", False, _lib.KERNEL_BF16, _lib.ACCUM_PLAIN),
+             ("f16_compensated", False, _lib.KERNEL_F16,
+              _lib.ACCUM_COMPENSATED),
+             ("fp32_compensated", False, _lib.KERNEL_NATIVE,
+              _lib.ACCUM_COMPENSATED),
+             ("fp64", True, _lib.KERNEL_NATIVE, _lib.ACCUM_PLAIN)]
+    rng = np.random.default_rng(31)
+    m = min(n, 200000)
+    sel = torch.as_tensor(np.sort(rng.choice(n, size=m, replace=False)),
+                          device="cuda")
+    sub = wl.subset(sel)
+    hd = host_dict(sub)
+    ref_sample = dict(hd)
+    for k in ("conv_func", "uu", "vv", "ww", "vis", "weight"):
+        ref_sample[k] = np.asarray(hd[k], np.float64)
+    _, _, g_oracle = O.grid_d(ref_sample, threads=host_threads())
+    results, grids = {}, {}
+    for name, dbl, kt, acc in modes:
+        real = torch.float64 if dbl else torch.float32
+        conv = wl.conv_func.double() if dbl else wl.conv_func
+        cube = fg.Cube(ws, wl.support, wl.oversample, wl.conv_size_half, conv,
+                       data_is_double=dbl, kernel_type=kt)
+        inp = [t.to(real) for t in (wl.uu, wl.vv, wl.ww, wl.vis, wl.weight)]
+        grid = torch.zeros(2 * g * g, dtype=real, device="cuda")
+        opts = fg.options(accum_mode=acc)
+
+        def step():
+            fg.grid_device(ws, cube, *inp, cell, wsc, g, grid, opts=opts,
+                           stream=s)
+        for _ in range(args.warmup):
+            step()
+        s.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(args.steps):
+            step()
+        e1.record(s)
+        e1.synchronize()
+        ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
+        grid.zero_()
+        step()
+        s.synchronize()
+        grids[name] = grid.double()
+        # the audited sample through the same mode
+        sg = torch.zeros(2 * g * g, dtype=real, device="cuda")
+        fg.grid_device(ws, cube, *[t.to(real) for t in
+                                   (sub.uu, sub.vv, sub.ww, sub.vis,
+                                    sub.weight)],
+                       cell, wsc, g, sg, opts=opts, stream=s)
+        s.synchronize()
+        results[name] = {
+            "ms_per_step": round(ms, 3),
+            "gvis_per_s": round(n * world / (ms * 1e-3) / 1e9, 4),
+            "rel_rms_vs_cpu_fp64_oracle_sample": O.rel_rms(
+                sg.double().cpu().numpy(), g_oracle)}
+        del inp, grid, sg
+        cube.close()
+        torch.cuda.empty_cache()
+    ref = grids["fp64"]
+    for name in results:
+        d = grids[name] - ref
+        results[name]["rel_rms_vs_fp64_full"] = float(
+            torch.sqrt((d * d).sum() / (ref * ref).sum()).item())
+        results[name]["max_cell_err_rel_to_max_cell"] = float(
+            (d.abs().max() / ref.abs().max()).item())
+    fp32 = results["fp32"]
+    return {"metric": METRIC, "value": fp32["gvis_per_s"], "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": fp32["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": DATA_DESC,
+            "config": {"workload": PRECISION_DESC if args.stations == 512
+                       else f"profiling case: {args.stations} stations x "
+                            f"{num_times} samples, otherwise as precision",
+                       "num_points": n, "grid_size": g,
+                       "l2": "inputs (9.4 GB/step) larger than L2; no flush"},
+            "modes": results,
+            "error_note": "rel_rms_vs_fp64_full: each mode's full-size grid "
+                          "against the GPU FP64 grid of the same inputs; "
+                          "rel_rms_vs_cpu_fp64_oracle_sample: a seeded "
+                          f"{m}-visibility sample gridded by each mode "
+                          "against the CPU FP64 oracle (bit-identical to the "
+                          "reference's oskar_grid_wproj_d)"}
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return None
@@ -1171,7 +1284,7 @@ def run_reference(args, world, rank):
         return {"impl": "reference",
                 "unavailable": "the reference has no degridder (Defines.h:48 "
                                "only reserves a DEGRIDDING switch)"}
-    if args.workload in ("batch128", "serving"):
+    if args.workload in ("batch128", "serving", "precision"):
         return {"impl": "reference",
                 "unavailable": f"the reference has no {args.workload} path; "
                                "its gridder is timed by the default workload"}
@@ -1225,7 +1338,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", choices=("plain_large", "batch128",
-                                           "serving", "weights", "degrid"),
+                                           "serving", "weights", "degrid",
+                                           "precision"),
                     default="plain_large",
                     help="plain_large (the benchmark job), batch128 (the "
                          "128-channel batching workload), serving (the "
@@ -1255,6 +1369,8 @@ def main():
             out = run_weights(args, world, rank, local)
         elif args.workload == "degrid":
             out = run_degrid(args, world, rank, local)
+        elif args.workload == "precision":
+            out = run_precision(args, world, rank, local)
         else:
             out = run_b200(args, world, rank, local)
         if rank == 0 and out is not None:

@@ -262,6 +262,30 @@ def plain_large(seed: int = 1, device="cpu", num_stations=512, num_times=300,
                    cell, w_scale, grid_size, gen, device, seed=seed)
 
 
+def precision_sweep(seed: int = 3, device="cpu", num_stations=512,
+                    num_times=3000, grid_size=4096, num_w_planes=128,
+                    oversample=8, freq_hz=150e6) -> Workload:
+    """Precision sweep, long integration: 512 stations uniform in a 5 km
+    disk (130,816 baselines, short ones dominating), 3000 samples 10 s apart
+    at 150 MHz, dec -30 deg (392,448,000 visibilities, concentrated near the
+    uv origin); sky as plain_small; grid 4096^2; 128 w-planes, support
+    4 -> 32, oversample 8.  The cell is chosen so the longest baseline plus
+    the largest support lands inside the grid."""
+    gen = torch.Generator().manual_seed(seed)
+    enu = stations_uniform_disk(num_stations, 5000.0, gen)
+    lat = dec = math.radians(-30.0)
+    uu, vv, ww = earth_rotation_uvw(baselines_xyz(enu, lat), num_times, 10.0,
+                                    freq_hz, dec, device)
+    vis = point_source_vis(uu, vv, ww, 10, math.radians(1.0), 0.1, gen)
+    support = support_ramp(num_w_planes, 4, 32)
+    w_scale = float((num_w_planes - 1) ** 2 / ww.abs().max().item())
+    uv_max = float(torch.maximum(uu.abs().max(), vv.abs().max()).item())
+    cell = (grid_size // 2 - int(support.max()) - 2) / (grid_size * uv_max)
+    csh = min_conv_size_half(support, oversample) + 1
+    return _finish("precision_sweep", uu, vv, ww, vis, support, oversample,
+                   csh, cell, w_scale, grid_size, gen, device, seed=seed)
+
+
 def batch_channels(seed: int = 2, device="cpu", num_channels=128,
                    num_stations=256, num_times=60, grid_size=2048,
                    num_w_planes=64, f_lo=50e6, f_hi=350e6, max_flag=0.7,
