@@ -262,7 +262,7 @@ def run_b200(args, world, rank, local):
     # timing events are recorded on it.
     stream = torch.cuda.Stream()
     torch.cuda.synchronize()
-    opts = fg.options()
+    opts = fg.options(classes_per_thread=args.cpt)
 
     def step():
         fg.grid_device(ws, cube, wl.uu, wl.vv, wl.ww, wl.vis, wl.weight,
@@ -1361,6 +1361,9 @@ def main():
                          "128-channel batching workload), serving (the "
                          "Poisson job stream) or weights (uniform "
                          "weighting over the benchmark job's uv points)")
+    ap.add_argument("--cpt", type=int, default=0,
+                    help="gridding classes per thread for every support "
+                         "(0: the tuned table)")
     ap.add_argument("--serving-jobs", type=int, default=2000)
     ap.add_argument("--serving-slots", type=int, default=4,
                     help="concurrent batches the server keeps on the GPU")

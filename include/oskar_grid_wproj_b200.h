@@ -181,7 +181,7 @@ typedef struct oskar_B200Options
     int kernel_type;     /* OSKAR_B200_KERNEL_* */
     int accum_mode;      /* OSKAR_B200_ACCUM_* */
     int apply_weight;    /* 0: ignore weight (reference); 1: vis and norm x weight */
-    int classes_per_thread; /* 0: autotuned table; 1, 2 or 4 forces it */
+    int classes_per_thread; /* 0: autotuned table; 1-6 or 8 forces it */
     int staging;         /* 0: auto; 1: TMA bulk copy to shared; 2: L1 reads */
     int compensate_radius; /* ACCUM_COMPENSATED: compensate only work whose
                             * footprint centre lies within this many cells of
