@@ -263,6 +263,17 @@ def run_b200(args, world, rank, local):
     stream = torch.cuda.Stream()
     torch.cuda.synchronize()
     opts = fg.options(classes_per_thread=args.cpt)
+    tuned = None
+    if args.autotune:
+        # classes per thread measured per support on a seeded 2 M sample
+        rng = np.random.default_rng(5)
+        idx = torch.as_tensor(np.sort(rng.choice(n, size=min(n, 2_000_000),
+                                                 replace=False)),
+                              device="cuda")
+        smp = wl.subset(idx)
+        tuned = ws.autotune(cube, smp.uu, smp.vv, smp.ww, smp.vis, cell, wsc,
+                            g, grid).tolist()
+        grid.zero_()
 
     def step():
         fg.grid_device(ws, cube, wl.uu, wl.vv, wl.ww, wl.vis, wl.weight,
@@ -359,6 +370,9 @@ def run_b200(args, world, rank, local):
            "grid_updates_per_step": updates,
            "roofline": roofline, "l2_atomic": l2_atomic, "stage_ms": stage_ms,
            "e2e": e2e, "gpu_launches": launches, "clocks": clk}
+    if tuned is not None:
+        sup = [int(x) for x in np.unique(wl.support)]
+        out["autotuned_classes_per_thread"] = {s: tuned[s] for s in sup}
     if rank == 0 and world == 1 and not args.no_cpu_baseline and \
             args.stations == 512:
         out["cpu_baseline"] = run_cpu_baseline(args, wl)
@@ -1361,6 +1375,9 @@ def main():
                          "128-channel batching workload), serving (the "
                          "Poisson job stream) or weights (uniform "
                          "weighting over the benchmark job's uv points)")
+    ap.add_argument("--autotune", action="store_true",
+                    help="measure classes per thread per support on a "
+                         "sample of the job before timing")
     ap.add_argument("--cpt", type=int, default=0,
                     help="gridding classes per thread for every support "
                          "(0: the tuned table)")

@@ -40,6 +40,8 @@ EXPORTED_SYMBOLS = (
     "oskar_b200_blocks_free",
     "oskar_b200_last_stats",
     "oskar_b200_set_stage_timing",
+    "oskar_b200_autotune",
+    "oskar_b200_tune_table",
     "oskar_b200_measure_atomic_rate",
     "oskar_b200_grid_f_static",
     "oskar_b200_server_create",
@@ -189,6 +191,10 @@ def load():
     lib.oskar_b200_last_stats.argtypes = [_P, C.POINTER(Stats)]
     lib.oskar_b200_build_info.restype = C.c_char_p
     lib.oskar_b200_set_stage_timing.argtypes = [_P, C.c_int]
+    lib.oskar_b200_autotune.argtypes = [
+        _P, _P, C.POINTER(Options), _SZ, _P, _P, _P, _P, C.c_double,
+        C.c_double, C.c_int, _P, _P]
+    lib.oskar_b200_tune_table.argtypes = [_P, _P, _P]
     lib.oskar_b200_measure_atomic_rate.argtypes = [
         _P, _P, C.c_int, C.c_int, C.POINTER(C.c_double)]
     lib.oskar_b200_grid_batch.argtypes = [_P, C.POINTER(Options), C.c_int,
@@ -221,6 +227,8 @@ def load():
                  "oskar_b200_grid", "oskar_b200_grid_batch",
                  "oskar_b200_place", "oskar_b200_last_stats",
                  "oskar_b200_set_stage_timing",
+    "oskar_b200_autotune",
+    "oskar_b200_tune_table",
                  "oskar_b200_measure_atomic_rate"):
         getattr(lib, name).restype = C.c_int
     _lib = lib

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "grid_romein.cuh"
 #include "internal.h"
 
 #define B200_STR2(x) #x
@@ -769,6 +770,50 @@ int oskar_b200_last_stats(oskar_B200Workspace* ws, oskar_B200Stats* stats)
                 cudaGetLastError();
                 *out[i] = 0.f;
             }
+    }
+    return OSKAR_B200_OK;
+}
+
+int oskar_b200_autotune(oskar_B200Workspace* ws, const oskar_B200Cube* cube,
+                        const oskar_B200Options* opt, size_t num_points,
+                        const void* uu, const void* vv, const void* ww,
+                        const void* vis, double cell_size_rad,
+                        double w_scale, int grid_size, void* grid,
+                        unsigned char* table_out)
+{
+    if (!ws || !cube) return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    oskar_B200Options defaults;
+    oskar_b200_options_init(&defaults);
+    if (!opt) opt = &defaults;
+    int st = check_options(opt, cube->data_is_double);
+    if (st) return st;
+    st = check_grid_args(num_points, uu, vv, ww, vis, nullptr, 0, grid_size,
+                         grid);
+    if (st) return st;
+    if (cube->device != ws->device) return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    DeviceGuard g(ws->device);
+    return run_autotune(ws, cube, opt, num_points, uu, vv, ww, vis,
+                        cell_size_rad, w_scale, grid_size, grid, table_out);
+}
+
+int oskar_b200_tune_table(oskar_B200Workspace* ws, const unsigned char* table,
+                          unsigned char* current)
+{
+    if (!ws) return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    if (table)
+    {
+        for (int s = 0; s < 128; ++s)
+            if (!((table[s] >= 1 && table[s] <= 6) || table[s] == 8))
+                return OSKAR_B200_ERR_INVALID_ARGUMENT;
+        memcpy(ws->tune, table, sizeof(ws->tune));
+        ws->tuned = 1;
+    }
+    if (current)
+    {
+        if (ws->tuned)
+            memcpy(current, ws->tune, sizeof(ws->tune));
+        else
+            default_tune_table(current);
     }
     return OSKAR_B200_OK;
 }

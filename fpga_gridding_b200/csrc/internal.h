@@ -90,12 +90,6 @@ struct DeviceBuffer
 // Events of the drop-in's pipelined upload: cube, grid and up to 14 chunks.
 constexpr int kIngestEvents = 16;
 
-// Grid-launch tuning for one support size (the "autotuner" table entry).
-struct TuneEntry
-{
-    unsigned char classes_per_thread;  // 1, 2 or 4
-};
-
 }  // namespace b200
 
 // Opaque public types.
@@ -136,6 +130,9 @@ struct oskar_B200Workspace
     int stage_timing = 0;
     int events_recorded = 0;
     cudaEvent_t events[5] = {};
+    // classes-per-thread table measured by oskar_b200_autotune
+    unsigned char tune[128] = {};
+    int tuned = 0;
 };
 
 struct oskar_B200Cube
@@ -281,6 +278,13 @@ double coord_scale_of(double frequency_hz);
 
 int selftest_bounded_wait(oskar_B200Workspace* ws, unsigned spins,
                           int* device_status);
+
+// ---- autotune.cu ------------------------------------------------------------
+int run_autotune(oskar_B200Workspace* ws, const oskar_B200Cube* cube,
+                 const oskar_B200Options* opt, size_t n, const void* uu,
+                 const void* vv, const void* ww, const void* vis,
+                 double cell_size_rad, double w_scale, int grid_size,
+                 void* grid, unsigned char* table_out);
 
 // dst[i] += src[i] for n reals (FP64 when is_double, else FP32).
 cudaError_t launch_add(void* dst, const void* src, size_t n, int is_double,

@@ -305,6 +305,8 @@ int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
     if ((opt->classes_per_thread >= 1 && opt->classes_per_thread <= 6) ||
         opt->classes_per_thread == 8)
         memset(ga.cpt, opt->classes_per_thread, sizeof(ga.cpt));
+    else if (ws->tuned)
+        memcpy(ga.cpt, ws->tune, sizeof(ga.cpt));
     else
         default_tune_table(ga.cpt);
     // Kernel values are read through L1 unless staging is asked for: on

@@ -191,6 +191,33 @@ class Workspace:
     def bytes(self) -> int:
         return int(self._lib.oskar_b200_workspace_bytes(self.handle))
 
+    def autotune(self, cube, uu, vv, ww, vis, cell_size_rad: float,
+                 w_scale: float, grid_size: int, grid,
+                 opts: Options | None = None) -> np.ndarray:
+        """Measures the fastest classes-per-thread per support on a sample
+        job (device tensors; `grid` is scratch) and keeps it for later
+        calls on this workspace.  Returns the table (index = support)."""
+        table = np.zeros(128, np.uint8)
+        check(self._lib.oskar_b200_autotune(
+            self.handle, cube.handle,
+            C.byref(opts) if opts is not None else None, uu.numel(),
+            _ptr(uu), _ptr(vv), _ptr(ww), _ptr(vis), float(cell_size_rad),
+            float(w_scale), grid_size, _ptr(grid),
+            table.ctypes.data_as(C.c_void_p)), "autotune")
+        return table
+
+    def tune_table(self, table=None) -> np.ndarray:
+        """Sets the classes-per-thread table (128 entries) if given; returns
+        the table in use."""
+        cur = np.zeros(128, np.uint8)
+        t = None
+        if table is not None:
+            t = np.ascontiguousarray(table, dtype=np.uint8)
+        check(self._lib.oskar_b200_tune_table(
+            self.handle, t.ctypes.data_as(C.c_void_p) if t is not None
+            else None, cur.ctypes.data_as(C.c_void_p)), "tune_table")
+        return cur
+
     def stats(self) -> Stats:
         s = Stats()
         check(self._lib.oskar_b200_last_stats(self.handle, C.byref(s)),

@@ -380,6 +380,27 @@ typedef struct oskar_B200Stats
 OSKAR_B200_EXPORT int oskar_b200_last_stats(oskar_B200Workspace* ws,
         oskar_B200Stats* stats);
 
+/* Autotuner: for each support size of `cube`, grids the sample job's
+ * visibilities on planes of that support alone with every built
+ * classes-per-thread choice (1-6, 8: how many footprint rows a thread of the
+ * gridding kernel owns), times the gridding kernel with CUDA events (best
+ * of three) and keeps the fastest per support in the workspace.  Supports
+ * with fewer than 2000 sample visibilities keep the cost-model choice.
+ * Later gridding calls on this workspace with classes_per_thread = 0 use
+ * the table.  Device arrays as oskar_b200_grid; `grid` is scratch (its
+ * contents are destroyed).  Synchronous.  table_out (host, 128 entries,
+ * indexed by support, may be NULL) receives the table. */
+OSKAR_B200_EXPORT int oskar_b200_autotune(oskar_B200Workspace* ws,
+        const oskar_B200Cube* cube, const oskar_B200Options* opt,
+        size_t num_points, const void* uu, const void* vv, const void* ww,
+        const void* vis, double cell_size_rad, double w_scale, int grid_size,
+        void* grid, unsigned char* table_out);
+/* Sets the workspace's classes-per-thread table (128 entries indexed by
+ * support, each 1-6 or 8; NULL leaves it) and/or copies the table in use
+ * into `current` (the cost model's until one is set or tuned). */
+OSKAR_B200_EXPORT int oskar_b200_tune_table(oskar_B200Workspace* ws,
+        const unsigned char* table, unsigned char* current);
+
 /* Statistics level of every later gridding call on this workspace:
  * 0 = none; bit 0 (1) = CUDA events between the stages (stage times in
  * oskar_B200Stats); bit 1 (2) = also count the grid atomics the gridding
