@@ -99,13 +99,22 @@ void workspace_free(oskar_B200Workspace* ws)
     DeviceGuard g(ws->device);
     if (ws->stream) cudaStreamSynchronize(ws->stream);
     if (ws->copy_stream) cudaStreamSynchronize(ws->copy_stream);
+    if (ws->d2h_stream) cudaStreamSynchronize(ws->d2h_stream);
     for (cudaEvent_t& e : ws->events)
         if (e) cudaEventDestroy(e);
     for (cudaEvent_t& e : ws->ingest_events)
         if (e) cudaEventDestroy(e);
+    for (cudaEvent_t& e : ws->band_events)
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t& e : ws->piece_events)
+        if (e) cudaEventDestroy(e);
     if (ws->copy_stream) cudaStreamDestroy(ws->copy_stream);
-    if (ws->jobs_event) cudaEventDestroy(ws->jobs_event);
-    if (ws->h_jobs) cudaFreeHost(ws->h_jobs);
+    if (ws->d2h_stream) cudaStreamDestroy(ws->d2h_stream);
+    for (int r = 0; r < kJobRing; ++r)
+    {
+        if (ws->jobs_event[r]) cudaEventDestroy(ws->jobs_event[r]);
+        if (ws->h_jobs[r]) cudaFreeHost(ws->h_jobs[r]);
+    }
     if (ws->h_counters) cudaFreeHost(ws->h_counters);
     if (ws->stream) cudaStreamDestroy(ws->stream);
     delete ws;  // DeviceBuffer destructors free device memory
@@ -211,10 +220,25 @@ int check_grid_args(size_t num_points, const void* uu, const void* vv,
     return OSKAR_B200_OK;
 }
 
-// Points per chunk of the drop-in's pipelined upload: chunk k is gridded
-// while chunk k + 1 crosses PCIe.
+// Points per chunk of the drop-in's pipelined upload ahead of the last
+// chunk: chunk k is gridded while chunk k + 1 crosses PCIe.  The first
+// chunks are smaller (kFirstChunk, doubling up to kIngestChunk) so that the
+// gridding starts soon after the call.
 constexpr size_t kIngestChunk = size_t(5) << 20;
+constexpr size_t kFirstChunk = size_t(5) << 18;
+// The last chunk holds about this fraction of the points.  It is gridded band
+// by band (rows of coarse tiles), and each band of the result goes back to
+// the host as soon as no later band can touch it, so the download of the
+// grid overlaps the gridding.  Its upload must end before the earlier chunks
+// are gridded: uploads run at about twice the gridding rate.
+constexpr double kTailFraction = 0.45;
 
+// The drop-in's device pipeline.  Streams: s grids, c uploads (the cube, the
+// chunks in order, then the caller's grid band by band), d adds each
+// finished band of the caller's grid to the accumulated contributions and
+// copies it back.  The caller's grid on the device (in_grid) is never
+// modified, so a job whose device status reports a failure is undone by
+// copying it back over the rows already returned.
 template <typename T>
 int drop_in(size_t num_w_planes, const int* support, int oversample,
             int conv_size_half, const T* conv_func, size_t num_points,
@@ -250,34 +274,71 @@ int drop_in(size_t num_w_planes, const int* support, int oversample,
     const size_t n = num_points;
     const size_t cube_elems = num_w_planes * (size_t)conv_size_half *
                               conv_size_half * 2;
-    const size_t grid_elems = 2 * (size_t)grid_size * grid_size;
-    const int chunks = n == 0 ? 1 : (int)std::min<size_t>(
-        kIngestEvents - 2, (n + kIngestChunk - 1) / kIngestChunk);
+    const size_t row_elems = 2 * (size_t)grid_size;
+    const size_t grid_elems = row_elems * grid_size;
+    const size_t tail = n <= kIngestChunk ? n : (size_t)((double)n *
+                                                         kTailFraction);
+    const size_t head = n - tail;
+    // Chunk k covers points [bound[k], bound[k + 1]); the last is the tail.
+    size_t bound[kIngestEvents];
+    int chunks = 0;
+    bound[0] = 0;
+    for (size_t at = 0, size = kFirstChunk; at < head;)
+    {
+        size_t e = std::min(head, at + size);
+        // no short remainder, and at most kIngestEvents - 2 head chunks
+        if (head - e < kFirstChunk || chunks == kIngestEvents - 3) e = head;
+        bound[++chunks] = e;
+        at = e;
+        size = std::min(kIngestChunk, 2 * size);
+    }
+    bound[++chunks] = n;
+    size_t rows_back = 0;   // rows of the caller's grid already overwritten
+    auto sync_all = [&]() {
+        cudaStreamSynchronize(s);
+        if (ws->copy_stream) cudaStreamSynchronize(ws->copy_stream);
+        if (ws->d2h_stream) cudaStreamSynchronize(ws->d2h_stream);
+    };
+    // Puts back the caller's rows already overwritten (when the device can
+    // still do it) and reports `status`.
+    auto fail = [&](int status) -> int {
+        sync_all();
+        cudaGetLastError();
+        if (rows_back &&
+            cudaMemcpyAsync(grid, ws->in_grid.ptr,
+                            rows_back * row_elems * sizeof(T),
+                            cudaMemcpyDeviceToHost, s) == cudaSuccess)
+            cudaStreamSynchronize(s);
+        cudaGetLastError();
+        return status;
+    };
 #define B200_CHECK(expr)                                            \
     do {                                                            \
         const cudaError_t e_ = (expr);                              \
-        if (e_ != cudaSuccess) { cudaStreamSynchronize(s);          \
-                                 if (ws->copy_stream)               \
-                                     cudaStreamSynchronize(         \
-                                         ws->copy_stream);          \
-                                 cudaGetLastError();                \
-                                 return status_from_cuda(e_); }     \
+        if (e_ != cudaSuccess) return fail(status_from_cuda(e_));   \
     } while (0)
-    // The uploads run on a second stream: the cube first, then the chunks
-    // of visibilities in order, then the caller's grid.  The gridding of
-    // chunk k waits only for chunk k, and it accumulates into a zeroed
-    // device grid, so the caller's grid crosses PCIe while the chunks grid;
-    // it is added in at the end.
     if (!ws->copy_stream)
         B200_CHECK(cudaStreamCreateWithFlags(&ws->copy_stream,
+                                             cudaStreamNonBlocking));
+    if (!ws->d2h_stream)
+        B200_CHECK(cudaStreamCreateWithFlags(&ws->d2h_stream,
                                              cudaStreamNonBlocking));
     for (cudaEvent_t& e : ws->ingest_events)
         if (!e) B200_CHECK(cudaEventCreateWithFlags(&e,
                                                     cudaEventDisableTiming));
+    for (int b = 0; b < kMaxBands; ++b)
+    {
+        if (!ws->band_events[b])
+            B200_CHECK(cudaEventCreateWithFlags(&ws->band_events[b],
+                                                cudaEventDisableTiming));
+        if (!ws->piece_events[b])
+            B200_CHECK(cudaEventCreateWithFlags(&ws->piece_events[b],
+                                                cudaEventDisableTiming));
+    }
     cudaStream_t c = ws->copy_stream;
+    cudaStream_t d = ws->d2h_stream;
     cudaEvent_t ev_cube = ws->ingest_events[0];
-    cudaEvent_t ev_grid = ws->ingest_events[1];
-    cudaEvent_t* ev_chunk = ws->ingest_events + 2;
+    cudaEvent_t* ev_chunk = ws->ingest_events + 1;
     B200_CHECK(ws->in_cube.ensure(cube_elems * sizeof(T)));
     B200_CHECK(ws->in_grid.ensure(grid_elems * sizeof(T)));
     B200_CHECK(ws->acc_grid.ensure(grid_elems * sizeof(T)));
@@ -291,7 +352,7 @@ int drop_in(size_t num_w_planes, const int* support, int oversample,
         B200_CHECK(ws->in_ww.ensure(n * sizeof(T)));
         B200_CHECK(ws->in_vis.ensure(2 * n * sizeof(T)));
     }
-    // The previous call's uploads were waited for before it returned.
+    // The previous call's copies were waited for before it returned.
     B200_CHECK(cudaMemcpyAsync(ws->in_cube.ptr, conv_func,
                                cube_elems * sizeof(T),
                                cudaMemcpyHostToDevice, c));
@@ -300,8 +361,7 @@ int drop_in(size_t num_w_planes, const int* support, int oversample,
     st = cube_init(tc.cube, device, num_w_planes, support, oversample,
                    conv_size_half, ws->in_cube.ptr, nullptr, dbl, dbl,
                    OSKAR_B200_KERNEL_NATIVE, s);
-    if (st) { cudaStreamSynchronize(s); cudaStreamSynchronize(c);
-              cudaGetLastError(); return st; }
+    if (st) return fail(st);
     B200_CHECK(cudaMemsetAsync(ws->in_norm.ptr, 0, sizeof(double) * slots,
                                s));
     B200_CHECK(cudaMemsetAsync(ws->acc_grid.ptr, 0, grid_elems * sizeof(T),
@@ -312,10 +372,14 @@ int drop_in(size_t num_w_planes, const int* support, int oversample,
     unsigned long long* d_status =
         reinterpret_cast<unsigned long long*>(d_norm + 1);
     unsigned long long* d_skip = d_status + 1;
+    T* acc = static_cast<T*>(ws->acc_grid.ptr);
+    T* in_grid = static_cast<T*>(ws->in_grid.ptr);
+    BandPlan plan{};
+    plan.events = ws->band_events;
     for (int k = 0; k < chunks; ++k)
     {
-        const size_t b = n * (size_t)k / (size_t)chunks;
-        const size_t e = n * (size_t)(k + 1) / (size_t)chunks;
+        const bool last = k == chunks - 1;
+        const size_t b = bound[k], e = bound[k + 1];
         const size_t m = e - b;
         T* du = static_cast<T*>(ws->in_uu.ptr) + b;
         T* dv = static_cast<T*>(ws->in_vv.ptr) + b;
@@ -334,34 +398,106 @@ int drop_in(size_t num_w_planes, const int* support, int oversample,
         }
         B200_CHECK(cudaEventRecord(ev_chunk[k], c));
         B200_CHECK(cudaStreamWaitEvent(s, ev_chunk[k], 0));
-        st = run_grid(ws, tc.cube, &opt, m, du, dv, dw, dz, nullptr,
-                      cell_size_rad, w_scale, grid_size, ws->acc_grid.ptr,
-                      d_skip + k, d_norm, s);
-        if (st) { cudaStreamSynchronize(s); cudaStreamSynchronize(c);
-                  cudaGetLastError(); return st; }
+        HostJob j{};
+        j.cube = tc.cube;
+        j.num_points = m;
+        j.uu = du;
+        j.vv = dv;
+        j.ww = dw;
+        j.vis = dz;
+        j.cell_size_rad = cell_size_rad;
+        j.w_scale = w_scale;
+        j.grid_size = grid_size;
+        j.grid = acc;
+        j.d_num_skipped = d_skip + k;
+        j.d_norm = d_norm;
+        st = run_batch(ws, &opt, 1, &j, s, false, last ? &plan : nullptr);
+        if (st) return fail(st);
         // Each chunk resets the workspace's status word: keep its bits.
         B200_CHECK(launch_status_or(ws, d_status, s));
     }
-    B200_CHECK(cudaMemcpyAsync(ws->in_grid.ptr, grid, grid_elems * sizeof(T),
-                               cudaMemcpyHostToDevice, c));
-    B200_CHECK(cudaEventRecord(ev_grid, c));
-    B200_CHECK(cudaStreamWaitEvent(s, ev_grid, 0));
-    B200_CHECK(launch_add(ws->in_grid.ptr, ws->acc_grid.ptr, grid_elems,
-                          dbl, ws->num_sms, s));
-    // Check the job before touching the caller's grid and norm.
+    // The caller's grid goes up band by band after the visibilities, in the
+    // order the bands are gridded.
+    const int nb = plan.num_bands;
+    const int rs = plan.row_shift;
+    const size_t G = (size_t)grid_size;
+    auto band_rows = [&](int b, size_t* r0, size_t* r1) {
+        *r0 = std::min(G, (size_t)b << rs);
+        *r1 = std::min(G, (size_t)(b + 1) << rs);
+    };
+    cudaEvent_t piece_of_band[kMaxBands] = {};
+    for (int i = 0; i < nb; ++i)
+    {
+        const int b = plan.order[i];
+        size_t r0, r1;
+        band_rows(b, &r0, &r1);
+        B200_CHECK(cudaMemcpyAsync(in_grid + r0 * row_elems,
+                                   grid + r0 * row_elems,
+                                   (r1 - r0) * row_elems * sizeof(T),
+                                   cudaMemcpyHostToDevice, c));
+        B200_CHECK(cudaEventRecord(ws->piece_events[i], c));
+        piece_of_band[b] = ws->piece_events[i];
+    }
+    // A row is final once every band whose footprints can reach it (within
+    // `halo` rows of the band) has been gridded.  After each band, the rows
+    // that just became final get the caller's values added and go back.
+    // (The caller's rows have all gone up before any of them comes back:
+    // each returned interval waits for the uploads of its own bands.)
+    std::vector<unsigned char> sent(G, 0);
+    bool done[kMaxBands] = {};
+    const long long H = 1ll << rs, halo = plan.halo;
+    for (int i = 0; i < nb; ++i)
+    {
+        const int b = plan.order[i];
+        done[b] = true;
+        const long long lo = std::max(0ll, (long long)b * H - halo);
+        const long long hi = std::min((long long)G, (long long)(b + 1) * H +
+                                                        halo);
+        bool waited = false;
+        for (long long r = lo; r < hi;)
+        {
+            auto final_row = [&](long long q) {
+                if (sent[q]) return false;
+                const long long b0 = std::max(0ll, (q - halo) >> rs);
+                const long long b1 = std::min((long long)nb - 1,
+                                              (q + halo) >> rs);
+                for (long long x = b0; x <= b1; ++x)
+                    if (!done[x]) return false;
+                return true;
+            };
+            if (!final_row(r)) { ++r; continue; }
+            long long e = r + 1;
+            while (e < hi && final_row(e)) ++e;
+            for (long long q = r; q < e; ++q) sent[q] = 1;
+            if (!waited)
+            {
+                B200_CHECK(cudaStreamWaitEvent(d, ws->band_events[i], 0));
+                waited = true;
+            }
+            for (long long x = r >> rs; x <= (e - 1) >> rs; ++x)
+                B200_CHECK(cudaStreamWaitEvent(d, piece_of_band[x], 0));
+            const size_t off = (size_t)r * row_elems;
+            const size_t cnt = (size_t)(e - r) * row_elems;
+            B200_CHECK(launch_add(acc + off, in_grid + off, cnt, dbl,
+                                  ws->num_sms, d));
+            rows_back = G;   // (fail() puts back every row from here on)
+            B200_CHECK(cudaMemcpyAsync(grid + off, acc + off,
+                                       cnt * sizeof(T),
+                                       cudaMemcpyDeviceToHost, d));
+            r = e;
+        }
+    }
     B200_CHECK(cudaStreamSynchronize(s));
     B200_CHECK(cudaStreamSynchronize(c));
+    B200_CHECK(cudaStreamSynchronize(d));
     B200_CHECK(cudaGetLastError());
     std::vector<unsigned long long> out(slots);
     B200_CHECK(cudaMemcpyAsync(out.data(), d_norm,
                                sizeof(double) * slots,
                                cudaMemcpyDeviceToHost, s));
     B200_CHECK(cudaStreamSynchronize(s));
-    if (out[1]) return out[1] & DEV_ERR_TIMEOUT ? OSKAR_B200_ERR_TIMEOUT
-                                                : OSKAR_B200_ERR_DEVICE_CHECK;
-    B200_CHECK(cudaMemcpyAsync(grid, ws->in_grid.ptr, grid_elems * sizeof(T),
-                               cudaMemcpyDeviceToHost, s));
-    B200_CHECK(cudaStreamSynchronize(s));
+    if (out[1]) return fail(out[1] & DEV_ERR_TIMEOUT ? OSKAR_B200_ERR_TIMEOUT
+                                                     : OSKAR_B200_ERR_DEVICE_CHECK);
 #undef B200_CHECK
     unsigned long long skipped = 0;
     for (int k = 0; k < chunks; ++k) skipped += out[2 + k];

@@ -447,7 +447,7 @@ romein_grid_kernel(const GridArgs a)
     TapVis<GT>* s_vis = reinterpret_cast<TapVis<GT>*>(
         smem + (STAGED ? a.block_smem_bytes : 0));
     __shared__ uint64_t s_bar;
-    __shared__ unsigned s_task;
+    __shared__ unsigned long long s_task;
     __shared__ uint32_t s_order[kGridThreads];
     __shared__ int s_run_begin[kMaxOffsets], s_run_end[kMaxOffsets];
     __shared__ unsigned char s_head[kTaskMax];
@@ -456,6 +456,14 @@ romein_grid_kernel(const GridArgs a)
     const V2* __restrict__ svis = static_cast<const V2*>(a.svis);
     unsigned long long* status = &a.counters[CNT_STATUS];
     const unsigned num_tasks = (unsigned)a.counters[CNT_TASKS];
+    unsigned long long first = 0, end = num_tasks;
+    unsigned long long* queue = &a.counters[CNT_TASK_NEXT];
+    if (a.range)
+    {
+        first = a.range[0];
+        end = min((unsigned long long)a.range[1], end);
+        queue = a.queue;
+    }
 
     if (STAGED && threadIdx.x == 0)
     {
@@ -468,8 +476,7 @@ romein_grid_kernel(const GridArgs a)
     unsigned flushes = 0;
     for (;;)
     {
-        if (threadIdx.x == 0)
-            s_task = (unsigned)atomicAdd(&a.counters[CNT_TASK_NEXT], 1ull);
+        if (threadIdx.x == 0) s_task = first + atomicAdd(queue, 1ull);
         if (threadIdx.x < kMaxOffsets)
         {
             s_run_begin[threadIdx.x] = 0;
@@ -478,14 +485,15 @@ romein_grid_kernel(const GridArgs a)
         // Also: every thread has finished with the previous task's records
         // and row block before they are overwritten below.
         __syncthreads();
-        const unsigned task = s_task;
-        if (task >= num_tasks) break;
+        if (s_task >= end) break;
+        const unsigned task = (unsigned)s_task;
         const uint32_t begin = a.task_start[task];
         int m = (int)(a.task_start[task + 1] - begin);
         if (m <= 0 || m > kTaskMax)
         {
             if (threadIdx.x == 0)
                 atomicOr(status, (unsigned long long)DEV_ERR_TASK);
+            __syncthreads();   // s_task is read before thread 0 rewrites it
             continue;
         }
         // The task's job: its cube, grid and geometry.
@@ -513,6 +521,7 @@ romein_grid_kernel(const GridArgs a)
         {
             if (threadIdx.x == 0)
                 atomicOr(status, (unsigned long long)DEV_ERR_TASK);
+            __syncthreads();   // s_task is read before thread 0 rewrites it
             continue;
         }
         const int cpt = d.support < kTuneMax ? a.cpt[d.support] : 5;

@@ -23,6 +23,11 @@ struct GridArgs
     int comp_radius;            // see oskar_B200Options::compensate_radius
     int count_flushes;          // count grid atomics (statistics)
     unsigned char cpt[kTuneMax];
+    // Optional task range [range[0], range[1]) with its own work-queue
+    // counter (one launch per band of grid rows); null: every task, queue
+    // head counters[CNT_TASK_NEXT].
+    const uint32_t* range;
+    unsigned long long* queue;
 };
 
 void default_tune_table(unsigned char* cpt);

@@ -87,8 +87,28 @@ struct DeviceBuffer
     }
 };
 
-// Events of the drop-in's pipelined upload: cube, grid and up to 14 chunks.
+// Events of the drop-in's pipelined upload: cube and up to 15 chunks.
 constexpr int kIngestEvents = 16;
+// Bands of grid rows (rows of coarse tiles, at most 16 per grid).
+constexpr int kMaxBands = 16;
+// Pinned host job tables per workspace (see oskar_B200Workspace::h_jobs).
+constexpr int kJobRing = 8;
+
+// Band-ordered gridding of one job: the gridding kernel runs once per band
+// of coarse-tile rows, bands taken in `order`, and events[i] (created by the
+// caller) is recorded on the stream after the i-th of them.  Band b covers
+// grid rows [b << row_shift, (b + 1) << row_shift); the footprints of its
+// tasks reach at most `halo` rows beyond it.  The order is outside-in
+// (0, last, 1, last - 1, ...): visibilities concentrate near the uv origin,
+// so the light outer bands finish first and the heavy central ones last.
+struct BandPlan
+{
+    cudaEvent_t* events;      // kMaxBands of them
+    int num_bands;            // set by run_batch
+    int row_shift;            // set by run_batch
+    int halo;                 // set by run_batch: the cube's largest support
+    int order[kMaxBands];     // set by run_batch
+};
 
 }  // namespace b200
 
@@ -105,22 +125,33 @@ struct oskar_B200Workspace
     // small arrays: counters, partial sums, per-job plane histograms and
     // skip counts, the job table
     b200::DeviceBuffer counters, partials, plane_counts, job_skipped, jobs;
-    // pinned host copy of the job table (the source of its upload), and the
-    // event after which the upload has read it
-    void* h_jobs = nullptr;
-    size_t h_jobs_bytes = 0;
-    cudaEvent_t jobs_event = nullptr;
-    int jobs_event_pending = 0;
+    // pinned host copies of the job table (the sources of its uploads), a
+    // ring of them so that a call rarely waits for an earlier call's upload,
+    // each with the event after which that upload has read it
+    void* h_jobs[b200::kJobRing] = {};
+    size_t h_jobs_bytes[b200::kJobRing] = {};
+    cudaEvent_t jobs_event[b200::kJobRing] = {};
+    int jobs_event_pending[b200::kJobRing] = {};
+    int jobs_slot = 0;
     // drop-in staging of the caller's host arrays
     b200::DeviceBuffer in_uu, in_vv, in_ww, in_vis, in_weight, in_grid,
         in_cube, in_norm;
     // error grid of ACCUM_COMPENSATED
     b200::DeviceBuffer comp_grid;
-    // drop-in pipelined upload: copy stream, its events (cube, grid, one per
+    // drop-in pipelined upload: copy stream, its events (cube, one per
     // chunk) and the zeroed grid the chunks accumulate into
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t ingest_events[b200::kIngestEvents] = {};
     b200::DeviceBuffer acc_grid;
+    // band-ordered last chunk: per band, the event after its gridding and
+    // the event after the upload of its rows of the caller's grid; the
+    // stream that adds finished rows to the caller's grid and copies them
+    // back; band_first[kMaxBands + 1] (uint32) then the bands' work-queue
+    // counters (uint64) at byte 128
+    cudaStream_t d2h_stream = nullptr;
+    cudaEvent_t band_events[b200::kMaxBands] = {};
+    cudaEvent_t piece_events[b200::kMaxBands] = {};
+    b200::DeviceBuffer bands;
     // pinned host mirror of the device counters (stats)
     void* h_counters = nullptr;
     unsigned long long last_points = 0;
@@ -187,7 +218,8 @@ int cube_build(oskar_B200Cube* cube, const void* d_conv_func,
 
 // ---- prep.cu / grid_romein.cu ---------------------------------------------
 // Sort key, most significant first:
-//   job | coarse tile (Morton) | w-plane | cell inside the tile (Morton)
+//   job | coarse tile (row-major: row, column) | w-plane |
+//   cell inside the tile (Morton)
 // with a skip flag above all of them.
 struct KeyLayout
 {
@@ -230,7 +262,7 @@ struct HostJob
 // `vis` written.
 int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
               int num_jobs, const HostJob* jobs, cudaStream_t st,
-              bool degrid = false);
+              bool degrid = false, BandPlan* bands = nullptr);
 
 // ---- degrid.cu ------------------------------------------------------------
 cudaError_t launch_degrid(const uint32_t* order, const uint32_t* sorted_keys,

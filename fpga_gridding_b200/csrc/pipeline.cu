@@ -70,8 +70,12 @@ double coord_scale_of(double frequency_hz)
 
 int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
               int num_jobs, const HostJob* jobs, cudaStream_t st,
-              bool degrid)
+              bool degrid, BandPlan* bands)
 {
+    // (the error grid is folded in after the last band: not band-ordered)
+    if (bands && (num_jobs != 1 || degrid || !bands->events ||
+                  opt->accum_mode == OSKAR_B200_ACCUM_COMPENSATED))
+        return OSKAR_B200_ERR_INVALID_ARGUMENT;
     const oskar_B200Cube* c0 = jobs[0].cube;
     const bool dbl = c0->data_is_double != 0;
     const size_t vsz = dbl ? sizeof(double) : sizeof(float);
@@ -104,25 +108,62 @@ int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
     KeyLayout kl;
     if (!make_key_layout(max_grid, max_planes, num_jobs, &kl))
         return OSKAR_B200_ERR_UNSUPPORTED;
+    if (bands)
+    {
+        bands->row_shift = kl.coarse_shift;
+        bands->num_bands = (max_grid + (1 << kl.coarse_shift) - 1) >>
+                           kl.coarse_shift;
+        bands->halo = c0->max_support;
+        if (bands->num_bands > kMaxBands) return OSKAR_B200_ERR_UNSUPPORTED;
+        for (int i = 0, lo = 0, hi = bands->num_bands - 1; lo <= hi; ++i)
+            bands->order[i] = (i & 1) ? hi-- : lo++;
+        // (the layout already holds: at most 16 coarse tiles per axis)
+        B200_TRY(ws->bands.ensure(256));
+    }
+    // Every band event is recorded on every successful path.
+    auto record_bands = [&]() -> cudaError_t {
+        if (!bands) return cudaSuccess;
+        for (int b = 0; b < bands->num_bands; ++b)
+        {
+            const cudaError_t e = cudaEventRecord(bands->events[b], st);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    };
     const size_t job_bytes = sizeof(JobDesc) * num_jobs;
     cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
     B200_TRY(cudaStreamIsCapturing(st, &capture));
     const bool capturing = capture != cudaStreamCaptureStatusNone;
-    // The previous call's upload of the job table must have read it before
-    // it is rewritten.  (A caller capturing a graph has synchronised.)
-    if (ws->jobs_event_pending && !capturing)
-        B200_TRY(cudaEventSynchronize(ws->jobs_event));
-    ws->jobs_event_pending = 0;
-    if (ws->h_jobs_bytes < job_bytes)
+    // The job table goes up from the next pinned buffer of the ring; the
+    // upload that last read that buffer must have happened before it is
+    // rewritten.  (A caller capturing a graph has synchronised.)
+    // Every buffer of the ring is (re)allocated together, so that a call
+    // being captured into a graph after one that sized them allocates
+    // nothing.
+    if (ws->h_jobs_bytes[0] < job_bytes)
     {
-        if (ws->h_jobs) cudaFreeHost(ws->h_jobs);
-        ws->h_jobs = nullptr;
-        ws->h_jobs_bytes = 0;
-        B200_TRY(cudaMallocHost(&ws->h_jobs, job_bytes));
-        ws->h_jobs_bytes = job_bytes;
+        for (int r = 0; r < kJobRing; ++r)
+        {
+            if (ws->jobs_event_pending[r] && !capturing)
+                B200_TRY(cudaEventSynchronize(ws->jobs_event[r]));
+            ws->jobs_event_pending[r] = 0;
+            if (ws->h_jobs[r]) cudaFreeHost(ws->h_jobs[r]);
+            ws->h_jobs[r] = nullptr;
+            ws->h_jobs_bytes[r] = 0;
+        }
+        for (int r = 0; r < kJobRing; ++r)
+        {
+            B200_TRY(cudaMallocHost(&ws->h_jobs[r], job_bytes));
+            ws->h_jobs_bytes[r] = job_bytes;
+        }
     }
+    const int slot = ws->jobs_slot;
+    ws->jobs_slot = (slot + 1) % kJobRing;
+    if (ws->jobs_event_pending[slot] && !capturing)
+        B200_TRY(cudaEventSynchronize(ws->jobs_event[slot]));
+    ws->jobs_event_pending[slot] = 0;
     if (comp) B200_TRY(ws->comp_grid.ensure(comp_floats * sizeof(float)));
-    JobDesc* hj = static_cast<JobDesc*>(ws->h_jobs);
+    JobDesc* hj = static_cast<JobDesc*>(ws->h_jobs[slot]);
     size_t first = 0, comp_off = 0;
     for (int j = 0; j < num_jobs; ++j)
     {
@@ -183,11 +224,11 @@ int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
         // Outside stream capture, remember when the upload has happened.
         if (!capturing)
         {
-            if (!ws->jobs_event)
-                B200_TRY(cudaEventCreateWithFlags(&ws->jobs_event,
+            if (!ws->jobs_event[slot])
+                B200_TRY(cudaEventCreateWithFlags(&ws->jobs_event[slot],
                                                   cudaEventDisableTiming));
-            B200_TRY(cudaEventRecord(ws->jobs_event, st));
-            ws->jobs_event_pending = 1;
+            B200_TRY(cudaEventRecord(ws->jobs_event[slot], st));
+            ws->jobs_event_pending[slot] = 1;
         }
     }
     const JobDesc* d_jobs = static_cast<const JobDesc*>(ws->jobs.ptr);
@@ -250,6 +291,7 @@ int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
     {
         B200_TRY(mark(2));
         B200_TRY(mark(3));
+        B200_TRY(record_bands());
         B200_TRY(mark(4));
         ws->events_recorded = timing ? 1 : 0;
         ws->last_launches = launches;
@@ -320,10 +362,36 @@ int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
         B200_TRY(cudaMemsetAsync(ws->comp_grid.ptr, 0,
                                  comp_floats * sizeof(float), st));
     int ctas = 0;
-    B200_TRY(mark(3));
-    B200_TRY(launch_grid(ga, dbl, c0->kernel_type, max_block, staged, comp,
-                         ws->num_sms, st, &ctas));
-    launches += 1;
+    if (bands)
+    {
+        uint32_t* band_first = static_cast<uint32_t*>(ws->bands.ptr);
+        unsigned long long* queues = reinterpret_cast<unsigned long long*>(
+            static_cast<unsigned char*>(ws->bands.ptr) + 128);
+        B200_TRY(launch_band_first(keys[which], ga.task_start, n, counters,
+                                   kl, bands->num_bands, band_first,
+                                   ws->num_sms, st));
+        B200_TRY(cudaMemsetAsync(queues, 0,
+                                 sizeof(unsigned long long) * kMaxBands, st));
+        launches += 1;
+        B200_TRY(mark(3));
+        for (int i = 0; i < bands->num_bands; ++i)
+        {
+            const int b = bands->order[i];
+            ga.range = band_first + b;
+            ga.queue = queues + b;
+            B200_TRY(launch_grid(ga, dbl, c0->kernel_type, max_block, staged,
+                                 comp, ws->num_sms, st, &ctas));
+            B200_TRY(cudaEventRecord(bands->events[i], st));
+            launches += 1;
+        }
+    }
+    else
+    {
+        B200_TRY(mark(3));
+        B200_TRY(launch_grid(ga, dbl, c0->kernel_type, max_block, staged,
+                             comp, ws->num_sms, st, &ctas));
+        launches += 1;
+    }
     if (comp)
     {
         B200_TRY(launch_fold_jobs(d_jobs, num_jobs, ws->num_sms, st));

@@ -70,7 +70,10 @@ __device__ __forceinline__ uint32_t make_key(const KeyLayout& k, int job,
     const uint32_t in_mask = (1u << k.coarse_shift) - 1u;
     const uint32_t fu = ((uint32_t)gu & in_mask) >> k.fine_shift;
     const uint32_t fv = ((uint32_t)gv & in_mask) >> k.fine_shift;
-    const uint32_t coarse = spread_bits(cu) | (spread_bits(cv) << 1);
+    // Coarse tiles in row-major order: tasks of one row of tiles are
+    // contiguous, so a band of grid rows is complete once its tasks and its
+    // neighbours' are (the drop-in streams such bands back to the host).
+    const uint32_t coarse = (cv << k.coarse_bits) | cu;
     const uint32_t fine = spread_bits(fu) | (spread_bits(fv) << 1);
     return ((uint32_t)job << k.job_shift) |
            (coarse << (k.plane_bits + 2 * k.fine_bits)) |
@@ -394,6 +397,58 @@ cudaError_t launch_tasks(const uint32_t* sorted_keys, size_t n,
     task_scatter_kernel<<<blocks, 256, 0, st>>>(flags, pos, sorted_keys, n,
                                                 job_shift, counters,
                                                 task_start, task_job);
+    return cudaGetLastError();
+}
+
+namespace {
+
+__device__ __forceinline__ int band_of_task(const uint32_t* keys,
+                                            const uint32_t* task_start,
+                                            unsigned t, int band_shift,
+                                            uint32_t band_mask)
+{
+    return (int)((keys[task_start[t]] >> band_shift) & band_mask);
+}
+
+// band_first[b] = first task whose band is >= b, for b in [0, num_bands];
+// tasks are in key order, so bands are non-decreasing along the list.
+__global__ void band_first_kernel(const uint32_t* __restrict__ sorted_keys,
+                                  const uint32_t* __restrict__ task_start,
+                                  const unsigned long long* __restrict__ counters,
+                                  int band_shift, uint32_t band_mask,
+                                  int num_bands, uint32_t* __restrict__ band_first)
+{
+    const unsigned nt = (unsigned)counters[CNT_TASKS];
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t <= nt;
+         t += (size_t)gridDim.x * blockDim.x)
+    {
+        int b = t < nt ? band_of_task(sorted_keys, task_start, (unsigned)t,
+                                      band_shift, band_mask)
+                       : num_bands;
+        b = b < num_bands ? b : num_bands;
+        int prev = t > 0 ? band_of_task(sorted_keys, task_start,
+                                        (unsigned)t - 1, band_shift, band_mask)
+                         : -1;
+        prev = prev < num_bands ? prev : num_bands;
+        for (int c = prev + 1; c <= b; ++c) band_first[c] = (uint32_t)t;
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_band_first(const uint32_t* sorted_keys,
+                              const uint32_t* task_start, size_t n,
+                              const unsigned long long* counters,
+                              const KeyLayout& kl, int num_bands,
+                              uint32_t* band_first, int num_sms,
+                              cudaStream_t st)
+{
+    const int shift = kl.plane_bits + 2 * kl.fine_bits + kl.coarse_bits;
+    const uint32_t mask = (1u << kl.coarse_bits) - 1u;
+    const unsigned blocks = grid_blocks(n + 1, num_sms, 8, 256);
+    band_first_kernel<<<blocks, 256, 0, st>>>(sorted_keys, task_start,
+                                              counters, shift, mask, num_bands,
+                                              band_first);
     return cudaGetLastError();
 }
 

@@ -154,6 +154,14 @@ cudaError_t launch_tasks(const uint32_t* sorted_keys, size_t n,
                          uint32_t* pos, void* scan_tmp, uint32_t* task_start,
                          uint32_t* task_job, int num_sms, cudaStream_t st,
                          int* launches);
+// Bands of a single job's task list: band b holds the tasks of coarse-tile
+// row b; band_first[b] (b <= num_bands) is its first task.
+cudaError_t launch_band_first(const uint32_t* sorted_keys,
+                              const uint32_t* task_start, size_t n,
+                              const unsigned long long* counters,
+                              const KeyLayout& kl, int num_bands,
+                              uint32_t* band_first, int num_sms,
+                              cudaStream_t st);
 cudaError_t launch_place(int data_is_double, int coord_mode, const void* uu,
                          const void* vv, const void* ww, size_t n,
                          const PlaceConsts& pc, const int* support,

@@ -9,7 +9,10 @@
  *    reset, norm and grid accumulate, weight is ignored (as the reference
  *    hard-codes weight 1.0, oskar_grid_wproj.c:80-81).  Like the reference
  *    they return void; a failure leaves grid/norm untouched and is readable
- *    with oskar_grid_wproj_b200_last_error() from the same thread.
+ *    with oskar_grid_wproj_b200_last_error() from the same thread.  (Rows of
+ *    grid are copied back while later rows still grid; after a failure
+ *    they are restored from the device copy of the caller's grid, so only
+ *    a fault that loses the CUDA context can leave some of them updated.)
  *
  * 2. An extended, asynchronous API on device-resident buffers with explicit
  *    stream, workspace, resident kernel cubes and precision options.  Every

@@ -119,6 +119,35 @@ def test_dropin_pipelined_chunks(oracle, single):
     assert abs(n2 - n1) <= max(TOL_D, w["uu"].size * 2.0 ** -53) * abs(n1)
 
 
+@pytest.mark.parametrize("single", [False, True])
+def test_dropin_bands_wider_than_band_height(oracle, single):
+    """Supports up to 70 on a 256^2 grid (bands of 64 rows): footprints
+    reach past the neighbouring band, so a band's rows go back to the host
+    only after the band two further on is gridded.  The drop-in still
+    matches the oracle, accumulating into the caller's grid."""
+    rng = np.random.default_rng(21)
+    g, os_, n = 256, 4, 6000
+    support = W.support_ramp(8, 8, 70)
+    csh = W.min_conv_size_half(support, os_) + 1
+    cube = W.analytic_kernel_cube(support, os_, csh).numpy()
+    pos = rng.uniform(-60.0, 60.0, (2, n))
+    w = dict(num_w_planes=8, support=support, oversample=os_,
+             conv_size_half=csh, conv_func=cube, uu=-pos[0] / g,
+             vv=pos[1] / g, ww=rng.uniform(-49.0, 49.0, n),
+             vis=rng.normal(size=2 * n), weight=np.ones(n),
+             cell_size_rad=1.0, w_scale=1.0, grid_size=g)
+    real = np.float32 if single else np.float64
+    base = rng.normal(size=2 * g * g).astype(real)
+    ref_in = promote(w) if single else w
+    s1, n1, g1 = oracle.grid_d(ref_in, grid_arr=base.astype(np.float64),
+                               norm=0.5, threads=8)
+    s2, n2, g2 = fg.grid_workload(w, single=single, grid=base.copy(),
+                                  norm=0.5)
+    assert 0 < s1 < n and s1 == s2
+    assert oracle.rel_rms(g2, g1) <= (TOL_F if single else TOL_D)
+    assert abs(n2 - n1) <= TOL_D * abs(n1)
+
+
 @pytest.mark.parametrize("name", golden_names())
 def test_golden_fixtures(name):
     inputs, out = load_golden(name)
