@@ -1042,7 +1042,36 @@ int dropin_workspace(oskar_B200Workspace** out)
                                  return status_from_cuda(e_); }     \
     } while (0)
 
+// Chunks of the weights drop-ins' pipelined transfers.
+int weight_chunks(size_t n)
+{
+    if (n == 0) return 1;
+    return (int)std::min<size_t>(kIngestEvents - 2,
+                                 (n + kIngestChunk - 1) / kIngestChunk);
+}
+
+// Streams and events of a weights drop-in (created on first use).
+cudaError_t weights_streams(oskar_B200Workspace* ws)
+{
+    cudaError_t e = cudaSuccess;
+    if (!ws->copy_stream)
+        e = cudaStreamCreateWithFlags(&ws->copy_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess && !ws->d2h_stream)
+        e = cudaStreamCreateWithFlags(&ws->d2h_stream, cudaStreamNonBlocking);
+    for (cudaEvent_t& ev : ws->ingest_events)
+        if (e == cudaSuccess && !ev)
+            e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    for (cudaEvent_t& ev : ws->band_events)
+        if (e == cudaSuccess && !ev)
+            e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    return e;
+}
+
 // oskar_grid_weights_write_{d,f} on host arrays: ordered (bit-exact) write.
+// The caller's grid goes up first, then the points in chunks on the copy
+// stream; each chunk is written into the grid as it lands, in order (so
+// every cell still sums its weights in input order, starting from the
+// caller's value), while the next chunk crosses PCIe.
 template <typename T>
 int weights_write_drop_in(size_t n, const T* uu, const T* vv,
                           const T* weight, double cell_size_rad,
@@ -1055,43 +1084,77 @@ int weights_write_drop_in(size_t n, const T* uu, const T* vv,
     st = dropin_workspace(&ws);
     if (st) return st;
     cudaStream_t s = ws->stream;
+    auto sync_all = [&]() {
+        cudaStreamSynchronize(s);
+        if (ws->copy_stream) cudaStreamSynchronize(ws->copy_stream);
+        if (ws->d2h_stream) cudaStreamSynchronize(ws->d2h_stream);
+        cudaGetLastError();
+    };
+#define B200_PCHECK(expr)                                           \
+    do {                                                            \
+        const cudaError_t e_ = (expr);                              \
+        if (e_ != cudaSuccess) { sync_all();                        \
+                                 return status_from_cuda(e_); }     \
+    } while (0)
+    B200_PCHECK(weights_streams(ws));
+    cudaStream_t c = ws->copy_stream;
     const size_t grid_bytes = (size_t)grid_size * grid_size * sizeof(T);
-    B200_WCHECK(ws->in_grid.ensure(grid_bytes));
-    B200_WCHECK(ws->in_norm.ensure(2 * sizeof(double)));
+    const int chunks = weight_chunks(n);
+    B200_PCHECK(ws->in_grid.ensure(grid_bytes));
+    B200_PCHECK(ws->in_norm.ensure(sizeof(unsigned long long) * chunks));
     if (n)
     {
-        B200_WCHECK(ws->in_uu.ensure(n * sizeof(T)));
-        B200_WCHECK(ws->in_vv.ensure(n * sizeof(T)));
-        B200_WCHECK(ws->in_weight.ensure(n * sizeof(T)));
-        B200_WCHECK(cudaMemcpyAsync(ws->in_uu.ptr, uu, n * sizeof(T),
-                                    cudaMemcpyHostToDevice, s));
-        B200_WCHECK(cudaMemcpyAsync(ws->in_vv.ptr, vv, n * sizeof(T),
-                                    cudaMemcpyHostToDevice, s));
-        B200_WCHECK(cudaMemcpyAsync(ws->in_weight.ptr, weight, n * sizeof(T),
-                                    cudaMemcpyHostToDevice, s));
+        B200_PCHECK(ws->in_uu.ensure(n * sizeof(T)));
+        B200_PCHECK(ws->in_vv.ensure(n * sizeof(T)));
+        B200_PCHECK(ws->in_weight.ensure(n * sizeof(T)));
     }
-    B200_WCHECK(cudaMemcpyAsync(ws->in_grid.ptr, grid, grid_bytes,
-                                cudaMemcpyHostToDevice, s));
+    B200_PCHECK(cudaMemcpyAsync(ws->in_grid.ptr, grid, grid_bytes,
+                                cudaMemcpyHostToDevice, c));
     unsigned long long* d_skip =
         static_cast<unsigned long long*>(ws->in_norm.ptr);
-    st = run_weights_write(ws, sizeof(T) == sizeof(double), 1, n,
-                           ws->in_uu.ptr, ws->in_vv.ptr, ws->in_weight.ptr,
-                           cell_size_rad, grid_size, ws->in_grid.ptr, d_skip,
-                           0.0, s);
-    if (st) { cudaStreamSynchronize(s); cudaGetLastError(); return st; }
-    B200_WCHECK(cudaStreamSynchronize(s));
+    for (int k = 0; k < chunks; ++k)
+    {
+        const size_t b = n * (size_t)k / (size_t)chunks;
+        const size_t m = n * (size_t)(k + 1) / (size_t)chunks - b;
+        T* du = static_cast<T*>(ws->in_uu.ptr) + b;
+        T* dv = static_cast<T*>(ws->in_vv.ptr) + b;
+        T* dw = static_cast<T*>(ws->in_weight.ptr) + b;
+        if (m)
+        {
+            B200_PCHECK(cudaMemcpyAsync(du, uu + b, m * sizeof(T),
+                                        cudaMemcpyHostToDevice, c));
+            B200_PCHECK(cudaMemcpyAsync(dv, vv + b, m * sizeof(T),
+                                        cudaMemcpyHostToDevice, c));
+            B200_PCHECK(cudaMemcpyAsync(dw, weight + b, m * sizeof(T),
+                                        cudaMemcpyHostToDevice, c));
+        }
+        B200_PCHECK(cudaEventRecord(ws->ingest_events[k], c));
+        B200_PCHECK(cudaStreamWaitEvent(s, ws->ingest_events[k], 0));
+        st = run_weights_write(ws, sizeof(T) == sizeof(double), 1, m, du, dv,
+                               dw, cell_size_rad, grid_size, ws->in_grid.ptr,
+                               d_skip + k, 0.0, s);
+        if (st) { sync_all(); return st; }
+    }
+    B200_PCHECK(cudaStreamSynchronize(s));
+    B200_PCHECK(cudaStreamSynchronize(c));
+    std::vector<unsigned long long> skips(chunks);
+    B200_PCHECK(cudaMemcpyAsync(skips.data(), d_skip,
+                                sizeof(unsigned long long) * chunks,
+                                cudaMemcpyDeviceToHost, s));
+    B200_PCHECK(cudaMemcpyAsync(grid, ws->in_grid.ptr, grid_bytes,
+                                cudaMemcpyDeviceToHost, s));
+    B200_PCHECK(cudaStreamSynchronize(s));
     unsigned long long skipped = 0;
-    B200_WCHECK(cudaMemcpyAsync(&skipped, d_skip, sizeof(skipped),
-                                cudaMemcpyDeviceToHost, s));
-    B200_WCHECK(cudaMemcpyAsync(grid, ws->in_grid.ptr, grid_bytes,
-                                cudaMemcpyDeviceToHost, s));
-    B200_WCHECK(cudaStreamSynchronize(s));
+    for (unsigned long long x : skips) skipped += x;
     *num_skipped = (size_t)skipped;
     return OSKAR_B200_OK;
 }
 
 // oskar_grid_weights_read_{d,f} on host arrays.  weight_out is uploaded as
-// well: the entries of skipped points keep their previous values.
+// well: the entries of skipped points keep their previous values.  The
+// caller's grid goes up first, then the points in chunks; each chunk is
+// read as it lands and its weight_out goes back on a third stream while
+// later chunks still cross PCIe.
 template <typename T>
 int weights_read_drop_in(size_t n, const T* uu, const T* vv,
                          const T* weight_in, T* weight_out,
@@ -1106,47 +1169,80 @@ int weights_read_drop_in(size_t n, const T* uu, const T* vv,
     st = dropin_workspace(&ws);
     if (st) return st;
     cudaStream_t s = ws->stream;
+    auto sync_all = [&]() {
+        cudaStreamSynchronize(s);
+        if (ws->copy_stream) cudaStreamSynchronize(ws->copy_stream);
+        if (ws->d2h_stream) cudaStreamSynchronize(ws->d2h_stream);
+        cudaGetLastError();
+    };
+    B200_PCHECK(weights_streams(ws));
+    cudaStream_t c = ws->copy_stream;
+    cudaStream_t d = ws->d2h_stream;
     const size_t grid_bytes = (size_t)grid_size * grid_size * sizeof(T);
-    B200_WCHECK(ws->in_grid.ensure(grid_bytes));
-    B200_WCHECK(ws->in_norm.ensure(2 * sizeof(double)));
+    const int chunks = weight_chunks(n);
+    B200_PCHECK(ws->in_grid.ensure(grid_bytes));
+    B200_PCHECK(ws->in_norm.ensure(sizeof(unsigned long long) * chunks));
     if (n)
     {
-        B200_WCHECK(ws->in_uu.ensure(n * sizeof(T)));
-        B200_WCHECK(ws->in_vv.ensure(n * sizeof(T)));
-        B200_WCHECK(ws->in_weight.ensure(n * sizeof(T)));
-        B200_WCHECK(ws->in_vis.ensure(n * sizeof(T)));
-        B200_WCHECK(cudaMemcpyAsync(ws->in_uu.ptr, uu, n * sizeof(T),
-                                    cudaMemcpyHostToDevice, s));
-        B200_WCHECK(cudaMemcpyAsync(ws->in_vv.ptr, vv, n * sizeof(T),
-                                    cudaMemcpyHostToDevice, s));
-        B200_WCHECK(cudaMemcpyAsync(ws->in_weight.ptr, weight_in,
-                                    n * sizeof(T), cudaMemcpyHostToDevice,
-                                    s));
-        B200_WCHECK(cudaMemcpyAsync(ws->in_vis.ptr, weight_out,
-                                    n * sizeof(T), cudaMemcpyHostToDevice,
-                                    s));
+        B200_PCHECK(ws->in_uu.ensure(n * sizeof(T)));
+        B200_PCHECK(ws->in_vv.ensure(n * sizeof(T)));
+        B200_PCHECK(ws->in_weight.ensure(n * sizeof(T)));
+        B200_PCHECK(ws->in_vis.ensure(n * sizeof(T)));
     }
-    B200_WCHECK(cudaMemcpyAsync(ws->in_grid.ptr, grid, grid_bytes,
-                                cudaMemcpyHostToDevice, s));
+    B200_PCHECK(cudaMemcpyAsync(ws->in_grid.ptr, grid, grid_bytes,
+                                cudaMemcpyHostToDevice, c));
     unsigned long long* d_skip =
         static_cast<unsigned long long*>(ws->in_norm.ptr);
-    st = run_weights_read(ws, sizeof(T) == sizeof(double), n, ws->in_uu.ptr,
-                          ws->in_vv.ptr, ws->in_weight.ptr, ws->in_vis.ptr,
-                          cell_size_rad, grid_size, ws->in_grid.ptr, d_skip,
-                          0.0, s);
-    if (st) { cudaStreamSynchronize(s); cudaGetLastError(); return st; }
-    B200_WCHECK(cudaStreamSynchronize(s));
-    unsigned long long skipped = 0;
-    B200_WCHECK(cudaMemcpyAsync(&skipped, d_skip, sizeof(skipped),
+    for (int k = 0; k < chunks; ++k)
+    {
+        const size_t b = n * (size_t)k / (size_t)chunks;
+        const size_t m = n * (size_t)(k + 1) / (size_t)chunks - b;
+        T* du = static_cast<T*>(ws->in_uu.ptr) + b;
+        T* dv = static_cast<T*>(ws->in_vv.ptr) + b;
+        T* dw = static_cast<T*>(ws->in_weight.ptr) + b;
+        T* dout = static_cast<T*>(ws->in_vis.ptr) + b;
+        if (m)
+        {
+            B200_PCHECK(cudaMemcpyAsync(du, uu + b, m * sizeof(T),
+                                        cudaMemcpyHostToDevice, c));
+            B200_PCHECK(cudaMemcpyAsync(dv, vv + b, m * sizeof(T),
+                                        cudaMemcpyHostToDevice, c));
+            B200_PCHECK(cudaMemcpyAsync(dw, weight_in + b, m * sizeof(T),
+                                        cudaMemcpyHostToDevice, c));
+            B200_PCHECK(cudaMemcpyAsync(dout, weight_out + b, m * sizeof(T),
+                                        cudaMemcpyHostToDevice, c));
+        }
+        B200_PCHECK(cudaEventRecord(ws->ingest_events[k], c));
+        B200_PCHECK(cudaStreamWaitEvent(s, ws->ingest_events[k], 0));
+        st = run_weights_read(ws, sizeof(T) == sizeof(double), m, du, dv, dw,
+                              dout, cell_size_rad, grid_size, ws->in_grid.ptr,
+                              d_skip + k, 0.0, s);
+        if (st) { sync_all(); return st; }
+        if (m)
+        {
+            // (every upload of this chunk happened before the event above,
+            // so its host rows are read before they are overwritten)
+            B200_PCHECK(cudaEventRecord(ws->band_events[k], s));
+            B200_PCHECK(cudaStreamWaitEvent(d, ws->band_events[k], 0));
+            B200_PCHECK(cudaMemcpyAsync(weight_out + b, dout, m * sizeof(T),
+                                        cudaMemcpyDeviceToHost, d));
+        }
+    }
+    B200_PCHECK(cudaStreamSynchronize(s));
+    B200_PCHECK(cudaStreamSynchronize(c));
+    B200_PCHECK(cudaStreamSynchronize(d));
+    std::vector<unsigned long long> skips(chunks);
+    B200_PCHECK(cudaMemcpyAsync(skips.data(), d_skip,
+                                sizeof(unsigned long long) * chunks,
                                 cudaMemcpyDeviceToHost, s));
-    if (n)
-        B200_WCHECK(cudaMemcpyAsync(weight_out, ws->in_vis.ptr,
-                                    n * sizeof(T), cudaMemcpyDeviceToHost,
-                                    s));
-    B200_WCHECK(cudaStreamSynchronize(s));
+    B200_PCHECK(cudaStreamSynchronize(s));
+    unsigned long long skipped = 0;
+    for (unsigned long long x : skips) skipped += x;
     *num_skipped = (size_t)skipped;
     return OSKAR_B200_OK;
 }
+
+#undef B200_PCHECK
 
 #undef B200_WCHECK
 
