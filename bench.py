@@ -721,10 +721,10 @@ def run_serving(args, world, rank, local):
     done = drain(set(range(num_jobs)))
     burst = num_jobs / (max(c["end_s"] for c in done.values()) - t0)
     # Poisson arrivals at 70% of capacity
-    rate = 0.7 * capacity
+    rate = args.serving_rate if args.serving_rate > 0 else 0.7 * capacity
     arrivals = np.cumsum(rng.exponential(1.0 / rate, size=num_jobs))
     mix_grids = {i: None for i in audited}
-    lat, batch_sizes, mem_peak = {}, [], 0
+    lat, waits, batch_sizes, mem_peak = {}, {}, [], 0
     start = srv.clock()
     nxt = 0
     pending = set()
@@ -739,6 +739,7 @@ def run_serving(args, world, rank, local):
             if c["status"] != 0:
                 raise RuntimeError(f"job {c['tag']} status {c['status']}")
             lat[c["tag"]] = c["end_s"] - c["submit_s"]
+            waits[c["tag"]] = c["start_s"] - c["submit_s"]
             batch_sizes.append(c["batch_size"])
             if c["tag"] in mix_grids:
                 # read after the stream (a copy here would hold up arrivals)
@@ -755,6 +756,14 @@ def run_serving(args, world, rank, local):
     lat_v = np.array([lat[i] for i in range(num_jobs)])
     iso_v = np.array([iso[i] for i in range(num_jobs)])
     ratio = lat_v / iso_v
+    # the jobs at or above the p99 latency: how long they queued for a slot
+    # and how long they ran, against their isolated latency
+    top = [i for i in range(num_jobs) if lat[i] >= np.percentile(lat_v, 99)]
+    tail = {"jobs": len(top),
+            "mean_visibilities": float(np.mean([jobs[i]["n"] for i in top])),
+            "mean_queue_s": float(np.mean([waits[i] for i in top])),
+            "mean_run_s": float(np.mean([lat[i] - waits[i] for i in top])),
+            "mean_isolated_s": float(np.mean([iso[i] for i in top]))}
     points = sum(j["n"] for j in jobs)
 
     # audit: mix vs alone for 5% of the jobs, FP64 oracle for the small ones
@@ -805,6 +814,7 @@ def run_serving(args, world, rank, local):
             "slowdown_vs_isolated": {"p50": pct(ratio, 50),
                                      "p99": pct(ratio, 99)},
             "p99_latency_over_p99_isolated": pct(lat_v, 99) / pct(iso_v, 99),
+            "p99_tail": tail,
             "mean_batch_size": float(np.mean(batch_sizes)),
             "server_memory_peak_bytes": mem_peak,
             "audit": {"jobs": len(audited),
@@ -1388,6 +1398,9 @@ def main():
                     help="gridding classes per thread for every support "
                          "(0: the tuned table)")
     ap.add_argument("--serving-jobs", type=int, default=2000)
+    ap.add_argument("--serving-rate", type=float, default=0.0,
+                    help="serving arrival rate in jobs/s (default: 70%% of "
+                         "the measured capacity)")
     ap.add_argument("--serving-slots", type=int, default=4,
                     help="concurrent batches the server keeps on the GPU")
     ap.add_argument("--serving-batch", type=int, default=32,

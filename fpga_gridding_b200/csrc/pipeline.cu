@@ -139,7 +139,10 @@ int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
     // rewritten.  (A caller capturing a graph has synchronised.)
     // Every buffer of the ring is (re)allocated together, so that a call
     // being captured into a graph after one that sized them allocates
-    // nothing.
+    // nothing; in steps of 64 KiB (256 jobs), since freeing pinned memory
+    // can wait for the whole device (a server growing its batches one job
+    // at a time stalled every slot on each step).
+    const size_t ring_bytes = (job_bytes + 65535) / 65536 * 65536;
     if (ws->h_jobs_bytes[0] < job_bytes)
     {
         for (int r = 0; r < kJobRing; ++r)
@@ -153,8 +156,8 @@ int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
         }
         for (int r = 0; r < kJobRing; ++r)
         {
-            B200_TRY(cudaMallocHost(&ws->h_jobs[r], job_bytes));
-            ws->h_jobs_bytes[r] = job_bytes;
+            B200_TRY(cudaMallocHost(&ws->h_jobs[r], ring_bytes));
+            ws->h_jobs_bytes[r] = ring_bytes;
         }
     }
     const int slot = ws->jobs_slot;
