@@ -242,8 +242,10 @@ __global__ void finalize_prep_kernel(const PrepArgs a)
     }
 }
 
-constexpr int kPermuteUnroll = 4;
-
+// One position per thread per step.  (Four per thread, their gathers
+// issued together, measured 1.57 -> 1.52 ms at plain_large but stalled the
+// server's mixed stream: p50 latency 4.9 -> 28-135 ms at 340 jobs/s, so
+// the plain loop stays.)
 template <typename T>
 __global__ void permute_kernel(const uint32_t* __restrict__ order,
                                const uint32_t* __restrict__ sorted_keys,
@@ -255,48 +257,23 @@ __global__ void permute_kernel(const uint32_t* __restrict__ order,
                                T* __restrict__ svis)
 {
     const size_t valid = n - counters[CNT_SKIPPED];
-    // kPermuteUnroll positions per thread per step, their random gathers
-    // issued together (a lone gather per thread leaves HBM mostly idle)
-    const size_t stride = (size_t)gridDim.x * blockDim.x;
-    for (size_t s0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-         s0 < valid; s0 += kPermuteUnroll * stride)
+    for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < valid;
+         s += (size_t)gridDim.x * blockDim.x)
     {
-        uint32_t idx[kPermuteUnroll], key[kPermuteUnroll];
-#pragma unroll
-        for (int u = 0; u < kPermuteUnroll; ++u)
+        const uint32_t i = order[s];
+        const JobDesc& jd = jobs[sorted_keys[s] >> job_shift];
+        const size_t local = i - jd.first;
+        const T* vis = static_cast<const T*>(jd.vis);
+        srec[s] = rec[i];
+        T re = vis[2 * local], im = vis[2 * local + 1];
+        if (apply_weight)
         {
-            const size_t s = s0 + u * stride;
-            idx[u] = s < valid ? order[s] : 0u;
-            key[u] = s < valid ? sorted_keys[s] : 0u;
+            const T w = static_cast<const T*>(jd.weight)[local];
+            re *= w;
+            im *= w;
         }
-        int4 r[kPermuteUnroll];
-        T re[kPermuteUnroll], im[kPermuteUnroll];
-#pragma unroll
-        for (int u = 0; u < kPermuteUnroll; ++u)
-        {
-            if (s0 + u * stride >= valid) continue;
-            const JobDesc& jd = jobs[key[u] >> job_shift];
-            const size_t local = idx[u] - jd.first;
-            const T* vis = static_cast<const T*>(jd.vis);
-            r[u] = rec[idx[u]];
-            re[u] = vis[2 * local];
-            im[u] = vis[2 * local + 1];
-            if (apply_weight)
-            {
-                const T w = static_cast<const T*>(jd.weight)[local];
-                re[u] *= w;
-                im[u] *= w;
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < kPermuteUnroll; ++u)
-        {
-            const size_t s = s0 + u * stride;
-            if (s >= valid) continue;
-            srec[s] = r[u];
-            svis[2 * s] = re[u];
-            svis[2 * s + 1] = im[u];
-        }
+        svis[2 * s] = re;
+        svis[2 * s + 1] = im;
     }
 }
 
