@@ -7,7 +7,7 @@ Python front end.  Importing the package does not load the library;
 calling any gridding function does, and fails loudly if it is missing.
 """
 from ._lib import EXPORTED_SYMBOLS, GridderError, LIB_PATH, load  # noqa: F401
-from .gridder import (Blocks, Cube, Workspace, degrid_device, grid_batch_device, grid_device,  # noqa: F401
+from .gridder import (Blocks, Cube, Workspace, degrid_device, degrid_host, grid_batch_device, grid_device,  # noqa: F401
                       grid_workload,
                       options, oskar_grid_weights_read_d,
                       oskar_grid_weights_read_f, oskar_grid_weights_write_d,

@@ -31,6 +31,7 @@ EXPORTED_SYMBOLS = (
     "oskar_b200_grid",
     "oskar_b200_grid_batch",
     "oskar_b200_degrid",
+    "oskar_b200_degrid_host",
     "oskar_b200_place",
     "oskar_b200_weights_write",
     "oskar_b200_weights_read",
@@ -179,6 +180,9 @@ def load():
     lib.oskar_b200_degrid.argtypes = [
         _P, _P, C.POINTER(Options), _SZ, _P, _P, _P, _P, C.c_double,
         C.c_double, C.c_int, _P, _P, _P, _P]
+    lib.oskar_b200_degrid_host.argtypes = [
+        _P, _P, C.POINTER(Options), _SZ, _P, _P, _P, _P, C.c_double,
+        C.c_double, C.c_int, _P, _P, C.POINTER(_SZ)]
     lib.oskar_b200_cube_free.argtypes = [_P]
     lib.oskar_b200_cube_bytes.argtypes = [_P]
     lib.oskar_b200_cube_bytes.restype = _SZ

@@ -1338,3 +1338,155 @@ int oskar_b200_weights_read(oskar_B200Workspace* ws, int data_is_double,
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Degridding of host arrays, with the copies overlapped
+// ---------------------------------------------------------------------------
+extern "C" {
+
+// The caller's grid goes up first (every chunk reads all of it), then the
+// visibilities' coordinates (and their current values: skipped ones keep
+// them) in chunks on the copy stream; each chunk is degridded as it lands
+// and its predicted visibilities go back on a third stream while later
+// chunks still cross PCIe.
+int oskar_b200_degrid_host(oskar_B200Workspace* ws, const oskar_B200Cube* cube,
+                           const oskar_B200Options* opt, size_t num_points,
+                           const void* uu, const void* vv, const void* ww,
+                           const void* weight, double cell_size_rad,
+                           double w_scale, int grid_size, const void* grid,
+                           void* vis, size_t* num_skipped)
+{
+    if (!ws || !cube || !num_skipped) return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    oskar_B200Options defaults;
+    oskar_b200_options_init(&defaults);
+    if (!opt) opt = &defaults;
+    int st = check_options(opt, cube->data_is_double);
+    if (st) return st;
+    if (opt->accum_mode != OSKAR_B200_ACCUM_PLAIN)
+        return OSKAR_B200_ERR_UNSUPPORTED;
+    st = check_grid_args(num_points, uu, vv, ww, vis, weight,
+                         opt->apply_weight, grid_size, grid);
+    if (st) return st;
+    if (cube->device != ws->device) return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    DeviceGuard g(ws->device);
+    cudaStream_t s = ws->stream;
+    auto sync_all = [&]() {
+        cudaStreamSynchronize(s);
+        if (ws->copy_stream) cudaStreamSynchronize(ws->copy_stream);
+        if (ws->d2h_stream) cudaStreamSynchronize(ws->d2h_stream);
+        cudaGetLastError();
+    };
+#define B200_DCHECK(expr)                                           \
+    do {                                                            \
+        const cudaError_t e_ = (expr);                              \
+        if (e_ != cudaSuccess) { sync_all();                        \
+                                 return status_from_cuda(e_); }     \
+    } while (0)
+    B200_DCHECK(weights_streams(ws));
+    cudaStream_t c = ws->copy_stream;
+    cudaStream_t d = ws->d2h_stream;
+    const size_t n = num_points;
+    const size_t T = cube->data_is_double ? sizeof(double) : sizeof(float);
+    const bool weighted = opt->apply_weight != 0;
+    const size_t grid_bytes = 2 * (size_t)grid_size * grid_size * T;
+    const int chunks = weight_chunks(n);
+    // [status of every chunk OR-ed, skip count of each chunk]
+    B200_DCHECK(ws->in_norm.ensure(sizeof(unsigned long long) *
+                                   (1 + (size_t)chunks)));
+    B200_DCHECK(ws->in_grid.ensure(grid_bytes));
+    if (n)
+    {
+        B200_DCHECK(ws->in_uu.ensure(n * T));
+        B200_DCHECK(ws->in_vv.ensure(n * T));
+        B200_DCHECK(ws->in_ww.ensure(n * T));
+        B200_DCHECK(ws->in_vis.ensure(2 * n * T));
+        if (weighted) B200_DCHECK(ws->in_weight.ensure(n * T));
+    }
+    unsigned long long* d_status =
+        static_cast<unsigned long long*>(ws->in_norm.ptr);
+    unsigned long long* d_skip = d_status + 1;
+    B200_DCHECK(cudaMemsetAsync(d_status, 0,
+                                sizeof(unsigned long long) * (1 + chunks), s));
+    B200_DCHECK(cudaMemcpyAsync(ws->in_grid.ptr, grid, grid_bytes,
+                                cudaMemcpyHostToDevice, c));
+    cudaEvent_t ev_grid = ws->ingest_events[kIngestEvents - 1];
+    B200_DCHECK(cudaEventRecord(ev_grid, c));
+    B200_DCHECK(cudaStreamWaitEvent(s, ev_grid, 0));
+    const unsigned char* h_uu = static_cast<const unsigned char*>(uu);
+    const unsigned char* h_vv = static_cast<const unsigned char*>(vv);
+    const unsigned char* h_ww = static_cast<const unsigned char*>(ww);
+    const unsigned char* h_w = static_cast<const unsigned char*>(weight);
+    unsigned char* h_vis = static_cast<unsigned char*>(vis);
+    for (int k = 0; k < chunks; ++k)
+    {
+        const size_t b = n * (size_t)k / (size_t)chunks;
+        const size_t m = n * (size_t)(k + 1) / (size_t)chunks - b;
+        unsigned char* du = static_cast<unsigned char*>(ws->in_uu.ptr) + b * T;
+        unsigned char* dv = static_cast<unsigned char*>(ws->in_vv.ptr) + b * T;
+        unsigned char* dw = static_cast<unsigned char*>(ws->in_ww.ptr) + b * T;
+        unsigned char* dz = static_cast<unsigned char*>(ws->in_vis.ptr) +
+                            2 * b * T;
+        unsigned char* dwt = weighted
+            ? static_cast<unsigned char*>(ws->in_weight.ptr) + b * T
+            : nullptr;
+        if (m)
+        {
+            B200_DCHECK(cudaMemcpyAsync(du, h_uu + b * T, m * T,
+                                        cudaMemcpyHostToDevice, c));
+            B200_DCHECK(cudaMemcpyAsync(dv, h_vv + b * T, m * T,
+                                        cudaMemcpyHostToDevice, c));
+            B200_DCHECK(cudaMemcpyAsync(dw, h_ww + b * T, m * T,
+                                        cudaMemcpyHostToDevice, c));
+            B200_DCHECK(cudaMemcpyAsync(dz, h_vis + 2 * b * T, 2 * m * T,
+                                        cudaMemcpyHostToDevice, c));
+            if (weighted)
+                B200_DCHECK(cudaMemcpyAsync(dwt, h_w + b * T, m * T,
+                                            cudaMemcpyHostToDevice, c));
+        }
+        B200_DCHECK(cudaEventRecord(ws->ingest_events[k], c));
+        B200_DCHECK(cudaStreamWaitEvent(s, ws->ingest_events[k], 0));
+        HostJob j{};
+        j.cube = cube;
+        j.num_points = m;
+        j.uu = du;
+        j.vv = dv;
+        j.ww = dw;
+        j.vis = dz;
+        j.weight = dwt;
+        j.cell_size_rad = cell_size_rad;
+        j.w_scale = w_scale;
+        j.grid_size = grid_size;
+        j.grid = ws->in_grid.ptr;
+        j.d_num_skipped = d_skip + k;
+        j.d_norm = nullptr;
+        j.frequency_hz = opt->frequency_hz;
+        st = run_batch(ws, opt, 1, &j, s, true);
+        if (st) { sync_all(); return st; }
+        // Each chunk resets the workspace's status word: keep its bits.
+        B200_DCHECK(launch_status_or(ws, d_status, s));
+        if (m)
+        {
+            B200_DCHECK(cudaEventRecord(ws->band_events[k], s));
+            B200_DCHECK(cudaStreamWaitEvent(d, ws->band_events[k], 0));
+            B200_DCHECK(cudaMemcpyAsync(h_vis + 2 * b * T, dz, 2 * m * T,
+                                        cudaMemcpyDeviceToHost, d));
+        }
+    }
+    B200_DCHECK(cudaStreamSynchronize(s));
+    B200_DCHECK(cudaStreamSynchronize(c));
+    B200_DCHECK(cudaStreamSynchronize(d));
+    std::vector<unsigned long long> out(1 + (size_t)chunks);
+    B200_DCHECK(cudaMemcpyAsync(out.data(), d_status,
+                                sizeof(unsigned long long) * out.size(),
+                                cudaMemcpyDeviceToHost, s));
+    B200_DCHECK(cudaStreamSynchronize(s));
+#undef B200_DCHECK
+    if (out[0]) return out[0] & DEV_ERR_TIMEOUT ? OSKAR_B200_ERR_TIMEOUT
+                                                : OSKAR_B200_ERR_DEVICE_CHECK;
+    unsigned long long skipped = 0;
+    for (int k = 0; k < chunks; ++k) skipped += out[1 + k];
+    *num_skipped = (size_t)skipped;
+    return OSKAR_B200_OK;
+}
+
+}  // extern "C"

@@ -320,6 +320,36 @@ def degrid_device(ws: Workspace, cube: Cube, uu, vv, ww, weight,
         _ptr(d_num_skipped), _stream_ptr(stream)), "oskar_b200_degrid")
 
 
+def degrid_host(ws: Workspace, cube: Cube, uu, vv, ww, weight,
+                cell_size_rad: float, w_scale: float, grid_size: int, grid,
+                vis, opts: Options | None = None) -> int:
+    """Synchronous degridding of host numpy arrays (float32 for an FP32
+    cube, float64 for FP64): `grid` is read, the kept visibilities' values
+    are written into `vis` (interleaved complex).  Returns the skip count.
+    The copies overlap the work (oskar_b200_degrid_host)."""
+    lib = load()
+    if opts is None:
+        opts = options()
+    real = np.float64 if cube.data_is_double else np.float32
+    for name, a in (("uu", uu), ("vv", vv), ("ww", ww), ("grid", grid),
+                    ("vis", vis)):
+        if not (isinstance(a, np.ndarray) and a.dtype == real and
+                a.flags["C_CONTIGUOUS"]):
+            raise TypeError(f"{name} must be a contiguous {real.__name__} "
+                            "numpy array")
+    w = None
+    if opts.apply_weight:
+        w = np.ascontiguousarray(weight, dtype=real)
+    skipped = C.c_size_t(0)
+    check(lib.oskar_b200_degrid_host(
+        ws.handle, cube.handle, C.byref(opts), uu.size, uu.ctypes.data,
+        vv.ctypes.data, ww.ctypes.data,
+        w.ctypes.data if w is not None else None, float(cell_size_rad),
+        float(w_scale), grid_size, grid.ctypes.data, vis.ctypes.data,
+        C.byref(skipped)), "oskar_b200_degrid_host")
+    return skipped.value
+
+
 def grid_batch_device(ws: Workspace, jobs, opts: Options | None = None,
                       stream=None) -> None:
     """Asynchronous batched gridding.  `jobs` is a sequence of dicts with

@@ -304,6 +304,21 @@ OSKAR_B200_EXPORT int oskar_b200_degrid(oskar_B200Workspace* ws,
         int grid_size, const void* grid, void* vis,
         unsigned long long* d_num_skipped, void* stream);
 
+/* Degridding of host arrays (no counterpart in the reference): the same
+ * result as oskar_b200_degrid, with uu, vv, ww, weight (read only with
+ * apply_weight), grid and vis in host memory (float arrays for an FP32
+ * cube, double for FP64) and the call synchronous.  The grid is uploaded
+ * first; the visibilities then cross PCIe in chunks of about 5 M that are
+ * degridded as they land, their predictions copied back while later
+ * chunks still upload.  Skipped visibilities keep their value in `vis`;
+ * *num_skipped receives their count.  On failure `vis` may be partly
+ * written.  Pinned host memory makes the copies several times faster. */
+OSKAR_B200_EXPORT int oskar_b200_degrid_host(oskar_B200Workspace* ws,
+        const oskar_B200Cube* cube, const oskar_B200Options* opt,
+        size_t num_points, const void* uu, const void* vv, const void* ww,
+        const void* weight, double cell_size_rad, double w_scale,
+        int grid_size, const void* grid, void* vis, size_t* num_skipped);
+
 /* Per-visibility placement exactly as the gridder computes it (device
  * pointers, int32 outputs, any may be NULL): grid cell, clamped w-plane,
  * oversample offsets, conjugation sign (+1/-1) and skip flag (0/1). */

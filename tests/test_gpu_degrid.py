@@ -139,3 +139,36 @@ def test_degrid_weights_and_reduced_precision(ws, oracle):
         err = rel_rms(v4, v3)
         print(f"kernel_type {kt}: degrid rel RMS vs FP64 oracle {err:.3e}")
         assert err <= tol
+
+
+@pytest.mark.parametrize("single", [True, False])
+def test_degrid_host_matches_device_call(ws, single):
+    """oskar_b200_degrid_host (host arrays, 5.6 M visibilities uploaded in
+    chunks that are degridded as they land) gives the device call's values
+    bit for bit, the same skip count, and leaves skipped entries of `vis`
+    as the caller had them."""
+    rng = np.random.default_rng(13)
+    real = np.float32 if single else np.float64
+    n, g, os_ = 5_600_000, 512, 4
+    support = W.support_ramp(8, 1, 3)
+    csh = W.min_conv_size_half(support, os_) + 1
+    cube_np = W.analytic_kernel_cube(support, os_, csh).numpy().astype(real)
+    # a few points fall off the grid edge (skipped)
+    pos = rng.uniform(-258.0, 258.0, (2, n))
+    h = dict(uu=(-pos[0] / g).astype(real), vv=(pos[1] / g).astype(real),
+             ww=rng.uniform(-49.0, 49.0, n).astype(real))
+    grid = rng.normal(size=2 * g * g).astype(real)
+    cube = fg.Cube(ws, support, os_, csh, cube_np, data_is_double=not single)
+    vis_host = np.full(2 * n, 3.5, dtype=real)
+    skipped = fg.degrid_host(ws, cube, h["uu"], h["vv"], h["ww"], None, 1.0,
+                             1.0, g, grid, vis_host)
+    d = lambda a: torch.as_tensor(a).cuda()
+    vis_dev = torch.full((2 * n,), 3.5, dtype=d(h["uu"]).dtype, device="cuda")
+    skip = torch.zeros(1, dtype=torch.int64, device="cuda")
+    fg.degrid_device(ws, cube, d(h["uu"]), d(h["vv"]), d(h["ww"]), None,
+                     1.0, 1.0, g, d(grid), vis_dev, skip)
+    torch.cuda.synchronize()
+    cube.close()
+    assert 0 < skipped < n and skipped == int(skip.item())
+    assert np.array_equal(vis_host, vis_dev.cpu().numpy())
+    assert np.count_nonzero(vis_host == 3.5) >= 2 * skipped
