@@ -42,8 +42,28 @@ struct __align__(16) TapVis
     unsigned origin;
     int mu, mv, tu;
     int cp, cn, rowbase, unused;
-    GT ar, ai, bi, br; // re += ar*Kre - ai*Kim; im += bi*Kre + br*Kim
+    // re += c0.x * Kre + c1.x * Kim;  im += c0.y * Kre + c1.y * Kim
+    typename Vec2<GT>::type c0, c1;
 };
+
+// acc += c0 * k.x + c1 * k.y, component-wise, one rounding per product
+// added (fma), in that order.  FP32: two packed fma.rn.f32x2 instead of
+// four scalar fma, the same roundings.
+__device__ __forceinline__ void cmac(float2& acc, const float2 c0,
+                                     const float2 c1, const float2 k)
+{
+    acc = __ffma2_rn(c0, make_float2(k.x, k.x), acc);
+    acc = __ffma2_rn(c1, make_float2(k.y, k.y), acc);
+}
+
+__device__ __forceinline__ void cmac(double2& acc, const double2 c0,
+                                     const double2 c1, const double2 k)
+{
+    acc.x = fma(c0.x, k.x, acc.x);
+    acc.x = fma(c1.x, k.y, acc.x);
+    acc.y = fma(c0.y, k.x, acc.y);
+    acc.y = fma(c1.y, k.y, acc.y);
+}
 
 template <typename GT>
 __device__ __forceinline__ TapVis<GT> derive(const int4 rec,
@@ -84,10 +104,10 @@ __device__ __forceinline__ TapVis<GT> derive(const int4 rec,
         sc = GT(0);
     }
     const GT vr = vis.x * sc, vi = vis.y * sc;
-    t.ar = vr;
-    t.ai = conj * vi;
-    t.bi = vi;
-    t.br = conj * vr;
+    t.c0.x = vr;
+    t.c0.y = vi;
+    t.c1.x = -(conj * vi);
+    t.c1.y = conj * vr;
     return t;
 }
 
@@ -317,7 +337,7 @@ __device__ __forceinline__ void process_task(const TapVis<GT>* __restrict__ s_vi
     for (int pass = 0; pass < lay.passes; ++pass)
     {
         const int b0 = pass * lay.groups * CPT + g;
-        GT are[CPT], aim[CPT];
+        typename Vec2<GT>::type acc[CPT];   // (re, im) of each row's cell
         unsigned cur[CPT];
         // Rows of this thread in this pass: b0 + q * groups, q < rows_here.
         int rows_here = (w - b0 + lay.groups - 1) / lay.groups;
@@ -334,7 +354,7 @@ __device__ __forceinline__ void process_task(const TapVis<GT>* __restrict__ s_vi
                 const unsigned rv = min((unsigned)(b + v.mv),
                                         (unsigned)(b + v.mv - w));
                 cur[q] = v.origin + ru + rv * (unsigned)grid_size;
-                are[q] = aim[q] = GT(0);
+                acc[q].x = acc[q].y = GT(0);
             }
         }
         for (int i = i0; i < i1; ++i)
@@ -366,22 +386,22 @@ __device__ __forceinline__ void process_task(const TapVis<GT>* __restrict__ s_vi
                 const auto k = kv[q];
                 const unsigned cell = cell0 + rvs[q] * (unsigned)grid_size;
                 const bool change = cell != cur[q];
-                flush(change, cur[q], are[q], aim[q]);
+                flush(change, cur[q], acc[q].x, acc[q].y);
                 if (COUNT) flushes += change;
-                are[q] = change ? GT(0) : are[q];
-                aim[q] = change ? GT(0) : aim[q];
+                acc[q].x = change ? GT(0) : acc[q].x;
+                acc[q].y = change ? GT(0) : acc[q].y;
                 cur[q] = cell;
-                are[q] = fma(v.ar, (GT)k.x, are[q]);
-                are[q] = fma(-v.ai, (GT)k.y, are[q]);
-                aim[q] = fma(v.bi, (GT)k.x, aim[q]);
-                aim[q] = fma(v.br, (GT)k.y, aim[q]);
+                typename Vec2<GT>::type kk;
+                kk.x = (GT)k.x;
+                kk.y = (GT)k.y;
+                cmac(acc[q], v.c0, v.c1, kk);
             }
         }
 #pragma unroll
         for (int q = 0; q < CPT; ++q)
         {
             if (q >= rows_here) break;
-            flush(true, cur[q], are[q], aim[q]);
+            flush(true, cur[q], acc[q].x, acc[q].y);
         }
         if (COUNT) flushes += rows_here > 0 ? rows_here : 0;
     }
@@ -561,10 +581,10 @@ romein_grid_kernel(const GridArgs a)
         {
             for (int q = t + 1; q < m && !s_head[q]; ++q)
             {
-                tv.ar += s_vis[q].ar;
-                tv.ai += s_vis[q].ai;
-                tv.bi += s_vis[q].bi;
-                tv.br += s_vis[q].br;
+                tv.c0.x += s_vis[q].c0.x;
+                tv.c0.y += s_vis[q].c0.y;
+                tv.c1.x += s_vis[q].c1.x;
+                tv.c1.y += s_vis[q].c1.y;
             }
         }
         __syncthreads();   // every run has been read
