@@ -1045,16 +1045,18 @@ int dropin_workspace(oskar_B200Workspace** out)
                                  return status_from_cuda(e_); }     \
     } while (0)
 
-// Chunks of the weights drop-ins' pipelined transfers.
-int weight_chunks(size_t n)
+// Chunks of the pipelined host-array calls (weights drop-ins, host
+// degridding): about kIngestChunk points each.
+int pipeline_chunks(size_t n)
 {
     if (n == 0) return 1;
     return (int)std::min<size_t>(kIngestEvents - 2,
                                  (n + kIngestChunk - 1) / kIngestChunk);
 }
 
-// Streams and events of a weights drop-in (created on first use).
-cudaError_t weights_streams(oskar_B200Workspace* ws)
+// Copy streams and events of the pipelined host-array calls (created on
+// first use).
+cudaError_t pipeline_streams(oskar_B200Workspace* ws)
 {
     cudaError_t e = cudaSuccess;
     if (!ws->copy_stream)
@@ -1099,10 +1101,10 @@ int weights_write_drop_in(size_t n, const T* uu, const T* vv,
         if (e_ != cudaSuccess) { sync_all();                        \
                                  return status_from_cuda(e_); }     \
     } while (0)
-    B200_PCHECK(weights_streams(ws));
+    B200_PCHECK(pipeline_streams(ws));
     cudaStream_t c = ws->copy_stream;
     const size_t grid_bytes = (size_t)grid_size * grid_size * sizeof(T);
-    const int chunks = weight_chunks(n);
+    const int chunks = pipeline_chunks(n);
     B200_PCHECK(ws->in_grid.ensure(grid_bytes));
     B200_PCHECK(ws->in_norm.ensure(sizeof(unsigned long long) * chunks));
     if (n)
@@ -1178,11 +1180,11 @@ int weights_read_drop_in(size_t n, const T* uu, const T* vv,
         if (ws->d2h_stream) cudaStreamSynchronize(ws->d2h_stream);
         cudaGetLastError();
     };
-    B200_PCHECK(weights_streams(ws));
+    B200_PCHECK(pipeline_streams(ws));
     cudaStream_t c = ws->copy_stream;
     cudaStream_t d = ws->d2h_stream;
     const size_t grid_bytes = (size_t)grid_size * grid_size * sizeof(T);
-    const int chunks = weight_chunks(n);
+    const int chunks = pipeline_chunks(n);
     B200_PCHECK(ws->in_grid.ensure(grid_bytes));
     B200_PCHECK(ws->in_norm.ensure(sizeof(unsigned long long) * chunks));
     if (n)
@@ -1382,14 +1384,14 @@ int oskar_b200_degrid_host(oskar_B200Workspace* ws, const oskar_B200Cube* cube,
         if (e_ != cudaSuccess) { sync_all();                        \
                                  return status_from_cuda(e_); }     \
     } while (0)
-    B200_DCHECK(weights_streams(ws));
+    B200_DCHECK(pipeline_streams(ws));
     cudaStream_t c = ws->copy_stream;
     cudaStream_t d = ws->d2h_stream;
     const size_t n = num_points;
     const size_t T = cube->data_is_double ? sizeof(double) : sizeof(float);
     const bool weighted = opt->apply_weight != 0;
     const size_t grid_bytes = 2 * (size_t)grid_size * grid_size * T;
-    const int chunks = weight_chunks(n);
+    const int chunks = pipeline_chunks(n);
     // [status of every chunk OR-ed, skip count of each chunk]
     B200_DCHECK(ws->in_norm.ensure(sizeof(unsigned long long) *
                                    (1 + (size_t)chunks)));
