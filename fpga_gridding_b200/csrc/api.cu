@@ -8,6 +8,7 @@
 #include <new>
 #include <vector>
 
+#include "band_rows.h"
 #include "common.cuh"
 #include "grid_romein.cuh"
 #include "internal.h"
@@ -441,54 +442,28 @@ int drop_in(size_t num_w_planes, const int* support, int oversample,
         B200_CHECK(cudaEventRecord(ws->piece_events[i], c));
         piece_of_band[b] = ws->piece_events[i];
     }
-    // A row is final once every band whose footprints can reach it (within
-    // `halo` rows of the band) has been gridded.  After each band, the rows
-    // that just became final get the caller's values added and go back.
-    // (The caller's rows have all gone up before any of them comes back:
-    // each returned interval waits for the uploads of its own bands.)
-    std::vector<unsigned char> sent(G, 0);
-    bool done[kMaxBands] = {};
-    const long long H = 1ll << rs, halo = plan.halo;
-    for (int i = 0; i < nb; ++i)
+    // After each band, the rows that just became final (no later band can
+    // reach them) get the caller's values added and go back.  (The caller's
+    // rows have all gone up before any of them comes back: each returned
+    // run waits for the uploads of its own bands.)
+    int waited_step = -1;
+    for (const FinalRows& f : final_rows(nb, plan.order, rs, plan.halo,
+                                         (long long)G))
     {
-        const int b = plan.order[i];
-        done[b] = true;
-        const long long lo = std::max(0ll, (long long)b * H - halo);
-        const long long hi = std::min((long long)G, (long long)(b + 1) * H +
-                                                        halo);
-        bool waited = false;
-        for (long long r = lo; r < hi;)
+        if (f.step != waited_step)
         {
-            auto final_row = [&](long long q) {
-                if (sent[q]) return false;
-                const long long b0 = std::max(0ll, (q - halo) >> rs);
-                const long long b1 = std::min((long long)nb - 1,
-                                              (q + halo) >> rs);
-                for (long long x = b0; x <= b1; ++x)
-                    if (!done[x]) return false;
-                return true;
-            };
-            if (!final_row(r)) { ++r; continue; }
-            long long e = r + 1;
-            while (e < hi && final_row(e)) ++e;
-            for (long long q = r; q < e; ++q) sent[q] = 1;
-            if (!waited)
-            {
-                B200_CHECK(cudaStreamWaitEvent(d, ws->band_events[i], 0));
-                waited = true;
-            }
-            for (long long x = r >> rs; x <= (e - 1) >> rs; ++x)
-                B200_CHECK(cudaStreamWaitEvent(d, piece_of_band[x], 0));
-            const size_t off = (size_t)r * row_elems;
-            const size_t cnt = (size_t)(e - r) * row_elems;
-            B200_CHECK(launch_add(acc + off, in_grid + off, cnt, dbl,
-                                  ws->num_sms, d));
-            rows_back = G;   // (fail() puts back every row from here on)
-            B200_CHECK(cudaMemcpyAsync(grid + off, acc + off,
-                                       cnt * sizeof(T),
-                                       cudaMemcpyDeviceToHost, d));
-            r = e;
+            B200_CHECK(cudaStreamWaitEvent(d, ws->band_events[f.step], 0));
+            waited_step = f.step;
         }
+        for (long long x = f.r0 >> rs; x <= (f.r1 - 1) >> rs; ++x)
+            B200_CHECK(cudaStreamWaitEvent(d, piece_of_band[x], 0));
+        const size_t off = (size_t)f.r0 * row_elems;
+        const size_t cnt = (size_t)(f.r1 - f.r0) * row_elems;
+        B200_CHECK(launch_add(acc + off, in_grid + off, cnt, dbl,
+                              ws->num_sms, d));
+        rows_back = G;   // (fail() puts back every row from here on)
+        B200_CHECK(cudaMemcpyAsync(grid + off, acc + off, cnt * sizeof(T),
+                                   cudaMemcpyDeviceToHost, d));
     }
     B200_CHECK(cudaStreamSynchronize(s));
     B200_CHECK(cudaStreamSynchronize(c));
