@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "band_rows.h"
+#include "ingest_plan.h"
 #include "common.cuh"
 #include "grid_romein.cuh"
 #include "internal.h"
@@ -221,22 +222,6 @@ int check_grid_args(size_t num_points, const void* uu, const void* vv,
     return OSKAR_B200_OK;
 }
 
-// Points per chunk of the drop-in's pipelined upload ahead of the last
-// chunk: chunk k is gridded while chunk k + 1 crosses PCIe.  The first
-// chunks are small (kFirstChunk, doubling up to kHeadChunkMax) so that the
-// gridding starts soon after the call; later ones large, as each chunk
-// pays the pipeline's fixed costs again (a 10 M cap measured 31.1 ms end
-// to end at plain_large against 31.4 ms with a 5 M cap).
-constexpr size_t kIngestChunk = size_t(5) << 20;
-constexpr size_t kFirstChunk = size_t(5) << 18;
-constexpr size_t kHeadChunkMax = size_t(10) << 20;
-// The last chunk holds about this fraction of the points.  It is gridded band
-// by band (rows of coarse tiles), and each band of the result goes back to
-// the host as soon as no later band can touch it, so the download of the
-// grid overlaps the gridding.  Its upload must end before the earlier chunks
-// are gridded: uploads run at about twice the gridding rate.
-constexpr double kTailFraction = 0.45;
-
 // The drop-in's device pipeline.  Streams: s grids, c uploads (the cube, the
 // chunks in order, then the caller's grid band by band), d adds each
 // finished band of the caller's grid to the accumulated contributions and
@@ -280,23 +265,10 @@ int drop_in(size_t num_w_planes, const int* support, int oversample,
                               conv_size_half * 2;
     const size_t row_elems = 2 * (size_t)grid_size;
     const size_t grid_elems = row_elems * grid_size;
-    const size_t tail = n <= kIngestChunk ? n : (size_t)((double)n *
-                                                         kTailFraction);
-    const size_t head = n - tail;
     // Chunk k covers points [bound[k], bound[k + 1]); the last is the tail.
+    // (One event per chunk after the cube's: at most kIngestEvents - 1.)
     size_t bound[kIngestEvents];
-    int chunks = 0;
-    bound[0] = 0;
-    for (size_t at = 0, size = kFirstChunk; at < head;)
-    {
-        size_t e = std::min(head, at + size);
-        // no short remainder, and at most kIngestEvents - 2 head chunks
-        if (head - e < kFirstChunk || chunks == kIngestEvents - 3) e = head;
-        bound[++chunks] = e;
-        at = e;
-        size = std::min(kHeadChunkMax, 2 * size);
-    }
-    bound[++chunks] = n;
+    const int chunks = ingest_chunks(n, kIngestEvents - 1, bound);
     size_t rows_back = 0;   // rows of the caller's grid already overwritten
     auto sync_all = [&]() {
         cudaStreamSynchronize(s);
