@@ -53,6 +53,7 @@ EXPORTED_SYMBOLS = (
     "oskar_b200_server_memory",
     "oskar_b200_server_free",
     "oskar_b200_selftest_bounded_wait",
+    "oskar_b200_testing_fail_allocation",
     "oskar_b200_build_info",
 )
 
@@ -207,6 +208,8 @@ def load():
         _SZ, _P, C.c_int, C.c_int, _P, _SZ, _P, _P, _P, _P, C.c_float,
         C.c_float, C.c_int, _P, _P, _P, _P]
     lib.oskar_b200_grid_f_static.restype = C.c_int
+    lib.oskar_b200_testing_fail_allocation.argtypes = [C.c_longlong]
+    lib.oskar_b200_testing_fail_allocation.restype = C.c_int
     lib.oskar_b200_selftest_bounded_wait.argtypes = [_P, C.c_uint,
                                                      C.POINTER(C.c_int)]
     lib.oskar_b200_selftest_bounded_wait.restype = C.c_int

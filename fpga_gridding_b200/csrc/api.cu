@@ -940,6 +940,13 @@ const char* oskar_b200_build_info(void)
 
 }  // extern "C"
 
+extern "C" int oskar_b200_testing_fail_allocation(long long after)
+{
+    if (after < -1) return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    g_alloc_countdown.store(after);
+    return OSKAR_B200_OK;
+}
+
 extern "C" int oskar_b200_selftest_bounded_wait(oskar_B200Workspace* ws,
                                                 unsigned spins,
                                                 int* device_status)

@@ -5,6 +5,7 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <vector>
 
 #include "oskar_grid_wproj_b200.h"
@@ -86,6 +87,9 @@ struct DeviceBuffer
         o.bytes = 0;
     }
 };
+
+// Injected device-allocation failures (testing aid), see pipeline.cu.
+extern std::atomic<long long> g_alloc_countdown;
 
 // Events of the drop-in's pipelined upload: cube and up to 15 chunks.
 constexpr int kIngestEvents = 16;

@@ -6,6 +6,7 @@
 //   -> one persistent Romein gridding launch over every task of every job.
 // A single oskar_b200_grid call is a batch of one job.
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <vector>
 
@@ -30,10 +31,20 @@ int status_from_cuda(cudaError_t e)
     }
 }
 
+// Allocation failures injected for tests (oskar_b200_testing_fail_allocation):
+// the number of device allocations still to succeed before one fails, or -1.
+std::atomic<long long> g_alloc_countdown{-1};
+
 cudaError_t DeviceBuffer::ensure(size_t n)
 {
     if (n <= bytes && ptr) return cudaSuccess;
     release();
+    long long left = g_alloc_countdown.load();
+    while (left >= 0 &&
+           !g_alloc_countdown.compare_exchange_weak(left, left - 1))
+    {
+    }
+    if (left == 0) return cudaErrorMemoryAllocation;
     const size_t granule = 2u << 20;
     const size_t want = n == 0 ? granule : (n + granule - 1) / granule * granule;
     cudaError_t e = cudaMalloc(&ptr, want);

@@ -535,6 +535,14 @@ OSKAR_B200_EXPORT int oskar_b200_server_free(oskar_B200Server* server);
 OSKAR_B200_EXPORT int oskar_b200_selftest_bounded_wait(
         oskar_B200Workspace* ws, unsigned spins, int* device_status);
 
+/* Testing aid for failure handling (the reference has no counterpart: it
+ * aborts on errors).  After `after` more device allocations by this library
+ * succeed, the next one fails as if the device were out of memory, once;
+ * -1 disarms.  Lets a test check that a call reports
+ * OSKAR_B200_ERR_OUT_OF_MEMORY and leaves the caller's outputs untouched
+ * without exhausting a shared GPU.  Process-wide; not for production use. */
+OSKAR_B200_EXPORT int oskar_b200_testing_fail_allocation(long long after);
+
 /* Library build description (arch, version). */
 OSKAR_B200_EXPORT const char* oskar_b200_build_info(void);
 

@@ -109,3 +109,13 @@ def test_invalid_arguments_rejected_before_any_device_work():
                            C.byref(norm), g.ctypes.data)
     assert lib.oskar_grid_wproj_b200_last_error() == _lib.ERR_INVALID_ARGUMENT
     assert norm.value == 1.0
+
+
+def test_fail_allocation_arms_and_rejects_bad_argument():
+    """The allocation-failure testing aid takes a count or -1 (disarm); it
+    touches no device."""
+    lib = _lib.load()
+    assert lib.oskar_b200_testing_fail_allocation(-2) == \
+        _lib.ERR_INVALID_ARGUMENT
+    assert lib.oskar_b200_testing_fail_allocation(3) == _lib.OK
+    assert lib.oskar_b200_testing_fail_allocation(-1) == _lib.OK
