@@ -240,6 +240,17 @@ def host_dict(wl32):
     return d
 
 
+def plain_config(stations, n, g, planes, oversample, world):
+    """The `config` of a plain_large line; both arms emit the same keys."""
+    workload = WORKLOAD_DESC if stations == 512 else (
+        f"profiling case: plain_large with {stations} stations "
+        f"({n} visibilities), otherwise identical")
+    return {"workload": workload, "num_points": n, "grid_size": g,
+            "num_w_planes": planes, "oversample": oversample,
+            "parallelism": f"replicas x{world}" if world > 1 else "single",
+            "l2": "inputs (0.8 GB/step) larger than L2; no flush"}
+
+
 def run_b200(args, world, rank, local):
     import ctypes as C
     import fpga_gridding_b200 as fg
@@ -325,11 +336,25 @@ def run_b200(args, world, rank, local):
     achieved = alg_bytes / (kernel_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peaks()
     traffic = profiled_traffic()
-    roofline = {"kernel": "romein_grid_kernel<float,float2,L1>", "bound": "hbm",
+    # The kernel's ceiling is not HBM: ncu shows instruction issue and the
+    # latency of its kernel-value loads limiting it with DRAM nearly idle
+    # (profiles/romein_grid_kernel_plain_large.md).  achieved/peak/frac
+    # still place its algorithmic bytes against the measured HBM copy rate;
+    # the L2-atomic roofline of its grid updates is in "l2_atomic".
+    roofline = {"kernel": "romein_grid_kernel<float,float2,L1>",
+                "bound": "issue",
+                "bound_evidence": "ncu small case: issue slots and "
+                                  "kernel-value load latency limit it; "
+                                  "DRAM throughput about 1 %",
                 "achieved": round(achieved, 2), "peak": peak,
                 "peak_source": peak_kind, "unit": "GB/s",
                 "frac": round(achieved / peak, 4),
                 "traffic": traffic,
+                "traffic_source": "ncu dram__bytes_read.sum + "
+                                  "dram__bytes_write.sum of one full-size "
+                                  "launch, copied from profiles/"
+                                  "romein_grid_kernel_plain_large.md (not "
+                                  "measured in this run)",
                 "algorithmic_bytes_per_launch": alg_bytes,
                 "kernel_ms": round(kernel_ms, 3)}
     # L2-atomic roofline: measured complex-FP32 red.v2 rate on an
@@ -353,19 +378,13 @@ def run_b200(args, world, rank, local):
     # End to end through the drop-in C entry point with pinned host buffers.
     e2e = None if args.no_e2e else run_e2e(args, wl, world)
 
-    workload = WORKLOAD_DESC if args.stations == 512 else (
-        f"profiling case: plain_large with {args.stations} stations "
-        f"({n} visibilities), otherwise identical")
     out = {"metric": METRIC, "value": round(value, 4), "unit": UNIT,
            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": round(ms_per_step, 3), "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
            "data": DATA_DESC,
-           "config": {"workload": workload, "num_points": n,
-                      "grid_size": g, "num_w_planes": wl.num_w_planes,
-                      "oversample": wl.oversample,
-                      "parallelism": f"replicas x{world}" if world > 1 else "single",
-                      "l2": "inputs (0.8 GB/step) larger than L2; no flush"},
+           "config": plain_config(args.stations, n, g, wl.num_w_planes,
+                                  wl.oversample, world),
            "grid_updates_per_s": updates_per_s,
            "grid_updates_per_step": updates,
            "roofline": roofline, "l2_atomic": l2_atomic, "stage_ms": stage_ms,
@@ -1326,6 +1345,8 @@ def run_reference(args, world, rank):
     use_ref = O.reference_lib() is not None
     wl = make_workload(0)
     hd = host_dict(wl)
+    config = plain_config(512, wl.num_points, wl.grid_size, wl.num_w_planes,
+                          wl.oversample, world)
     del wl
     torch.cuda.empty_cache() if torch.cuda.is_available() else None
     per_step_s = max(2.0, min(10.0, 120.0 / max(1, args.steps + args.warmup)))
@@ -1347,9 +1368,7 @@ def run_reference(args, world, rank):
             "ms_per_step": round(1e3 * tot_secs / args.steps, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": DATA_DESC,
-            "config": {"workload": WORKLOAD_DESC,
-                       "num_points": len(hd["uu"]),
-                       "grid_size": hd["grid_size"]},
+            "config": config,
             "grid_updates_per_s": tot_taps / tot_secs,
             "cpu_baseline": {"value": round(value, 6), "unit": UNIT,
                              "cores": t, "kind": kind,

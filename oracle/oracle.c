@@ -157,6 +157,58 @@ void orc_grid_wproj_d(size_t num_w_planes, const int* support, int oversample,
     }
 }
 
+/* Weighted FP64 gridding: the weighting of the reference's tiled CUDA
+ * gridder (oskar_grid_wproj_gpu.cu.old:718-724 and :965-978 scale each
+ * visibility by its weight before the tap loop; :799 and :1261 add the
+ * tap sum times the weight to the norm), on the FP64 placement and tap
+ * arithmetic of oskar_grid_wproj_d above.  With unit weights it equals
+ * orc_grid_wproj_d bit for bit. */
+void orc_grid_wproj_weighted_d(size_t num_w_planes, const int* support,
+        int oversample, int conv_size_half, const double* conv_func,
+        size_t num_points, const double* uu, const double* vv,
+        const double* ww, const double* vis, const double* weight,
+        double cell_size_rad, double w_scale, int grid_size,
+        size_t* num_skipped, double* norm, double* grid)
+{
+    const size_t plane_elems = (size_t)conv_size_half * conv_size_half;
+    const double grid_scale = grid_size * cell_size_rad;
+    size_t n;
+    *num_skipped = 0;
+    for (n = 0; n < num_points; ++n)
+    {
+        Place p;
+        double tap_sum = 0.0;
+        int dv, du;
+        place_d(num_w_planes, support, oversample, grid_scale, grid_size,
+                w_scale, uu[n], vv[n], ww[n], &p);
+        if (p.skipped) { *num_skipped += 1; continue; }
+        {
+            const double w = weight[n];
+            const double a_re = vis[2 * n] * w, a_im = vis[2 * n + 1] * w;
+            const double sgn = (double)p.conj;
+            const size_t plane_base = p.plane * plane_elems;
+            for (dv = -p.support; dv <= p.support; ++dv)
+            {
+                const size_t row = (size_t)(p.gv + dv) * (size_t)grid_size;
+                const size_t krow = plane_base + (size_t)abs(p.off_v +
+                        dv * oversample) * (size_t)conv_size_half;
+                for (du = -p.support; du <= p.support; ++du)
+                {
+                    const size_t ki = 2 * (krow +
+                            (size_t)abs(p.off_u + du * oversample));
+                    const size_t gi = 2 * (row + (size_t)(p.gu + du));
+                    const double k_re = conv_func[ki];
+                    const double k_im = conv_func[ki + 1] * sgn;
+                    grid[gi]     += (a_re * k_re - a_im * k_im);
+                    grid[gi + 1] += (a_im * k_re + a_re * k_im);
+                    tap_sum += k_re;
+                }
+            }
+            *norm += tap_sum * w;
+        }
+    }
+}
+
 void orc_grid_wproj_f(size_t num_w_planes, const int* support, int oversample,
         int conv_size_half, const float* conv_func, size_t num_points,
         const float* uu, const float* vv, const float* ww,

@@ -37,6 +37,17 @@ void orc_grid_wproj_d(size_t num_w_planes, const int* support, int oversample,
  * num_points.  The shipped reference loops a fixed 10000 points and prints
  * progress (oskar_grid_wproj.c:154-157); those two debugging lines are the
  * only deviation.  All coordinate arithmetic is float, as in the reference. */
+/* FP64 gridding with each visibility scaled by its weight and the norm
+ * adding tap sum x weight: the weighting of the reference's tiled CUDA
+ * gridder (oskar_grid_wproj_gpu.cu.old:718-724, :799), on the arithmetic
+ * of oskar_grid_wproj_d.  Unit weights give orc_grid_wproj_d exactly. */
+void orc_grid_wproj_weighted_d(size_t num_w_planes, const int* support,
+        int oversample, int conv_size_half, const double* conv_func,
+        size_t num_points, const double* uu, const double* vv,
+        const double* ww, const double* vis, const double* weight,
+        double cell_size_rad, double w_scale, int grid_size,
+        size_t* num_skipped, double* norm, double* grid);
+
 void orc_grid_wproj_f(size_t num_w_planes, const int* support, int oversample,
         int conv_size_half, const float* conv_func, size_t num_points,
         const float* uu, const float* vv, const float* ww,

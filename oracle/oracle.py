@@ -71,6 +71,8 @@ def oracle_lib():
         lib.orc_vis_place_d.argtypes = pl + [C.c_double, C.c_double, C.c_int] + [_P] * 8
         lib.orc_vis_place_f.argtypes = pl + [C.c_float, C.c_float, C.c_int] + [_P] * 8
         lib.orc_vis_place_d.restype = lib.orc_vis_place_f.restype = None
+        lib.orc_grid_wproj_weighted_d.argtypes = _GRID_ARGS_D
+        lib.orc_grid_wproj_weighted_d.restype = None
         lib.orc_grid_wproj_d_banded.argtypes = _GRID_ARGS_D + [C.c_int]
         lib.orc_grid_wproj_f_banded.argtypes = _GRID_ARGS_F + [C.c_int]
         lib.orc_count_taps_d.argtypes = [_SZ, _P, C.c_int, _SZ, _P, _P, _P,
@@ -192,6 +194,13 @@ def grid_d(w, grid_arr=None, norm=0.0, threads=None):
     lib = oracle_lib()
     fn = lib.orc_grid_wproj_d if threads is None else lib.orc_grid_wproj_d_banded
     return grid(fn, w, np.float64, grid_arr, norm, threads)
+
+
+def grid_weighted_d(w, grid_arr=None, norm=0.0):
+    """Oracle FP64 gridding with each visibility scaled by its weight (the
+    reference tiled CUDA gridder's weighting)."""
+    return grid(oracle_lib().orc_grid_wproj_weighted_d, w, np.float64,
+                grid_arr, norm)
 
 
 def grid_f(w, grid_arr=None, norm=0.0, threads=None):

@@ -2,6 +2,8 @@
 concurrently and in merged batches; each result equals the same job gridded
 alone (and the FP64 oracle), the HBM budget is respected, and a job that can
 never fit is rejected."""
+import time
+
 import numpy as np
 import pytest
 import torch
@@ -39,9 +41,14 @@ def _oracle_grid(oracle, w):
     return oracle.grid_d(d, threads=8)
 
 
-def _collect(srv, n):
+def _collect(srv, n, deadline_s=300.0):
+    """Every completion of n jobs; fails the test (instead of polling
+    forever) if they have not all arrived within deadline_s."""
     done = {}
+    t_end = time.monotonic() + deadline_s
     while len(done) < n:
+        assert time.monotonic() < t_end, \
+            f"{n - len(done)} of {n} jobs not completed after {deadline_s} s"
         for c in srv.poll(timeout=1.0):
             done[c["tag"]] = c
     return done
@@ -104,7 +111,9 @@ def test_budget_is_respected_and_impossible_job_rejected():
     srv.submit(99, cubes[0], j["uu"], j["vv"], j["ww"], j["vis"],
                j["weight"], j["cell"], j["wsc"], 8192)
     done = {}
+    t_end = time.monotonic() + 300.0
     while len(done) < len(jobs) + 1:
+        assert time.monotonic() < t_end, "jobs not completed after 300 s"
         for c in srv.poll(timeout=1.0):
             done[c["tag"]] = c
             used, cap = srv.memory()

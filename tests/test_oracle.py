@@ -222,3 +222,37 @@ def test_parallel_timing_harness_sums_to_serial(oracle, small):
     assert secs > 0 and sk == s1
     assert abs(nrm - n1) <= 1e-12 * abs(n1)
     assert oracle.rel_rms(grid, g1) < 1e-13
+
+
+def test_weighted_oracle_with_unit_weights_is_the_reference(oracle, ref):
+    """The weighted restatement (the reference tiled CUDA gridder's
+    weighting) with unit weights is the reference's own oskar_grid_wproj_d,
+    bit for bit."""
+    w = W.plain_small(num_stations=24, num_times=40, grid_size=256,
+                      num_w_planes=8).numpy()
+    w["weight"] = np.ones_like(w["weight"])
+    s1, n1, g1 = oracle.grid(ref.ref_oskar_grid_wproj_d, w, np.float64)
+    s2, n2, g2 = oracle.grid_weighted_d(w)
+    assert (s1, n1) == (s2, n2)
+    assert np.array_equal(g1, g2)
+
+
+def test_weighted_oracle_scales_each_visibility(oracle):
+    """Random weights: the grid equals the unweighted gridder's on the
+    visibilities times their weights (the same products, the same order);
+    weights of exactly 2 double the norm exactly."""
+    w = W.plain_small(num_stations=24, num_times=40, grid_size=256,
+                      num_w_planes=8).numpy()
+    rng = np.random.default_rng(4)
+    w["weight"] = rng.uniform(0.25, 4.0, len(w["uu"]))
+    s1, n1, g1 = oracle.grid_weighted_d(w)
+    scaled = dict(w)
+    scaled["vis"] = (w["vis"].reshape(-1, 2) *
+                     w["weight"][:, None]).reshape(-1)
+    s2, _, g2 = oracle.grid_d(scaled)
+    assert s1 == s2 and np.array_equal(g1, g2)
+    two = dict(w)
+    two["weight"] = np.full(len(w["uu"]), 2.0)
+    _, n_two, _ = oracle.grid_weighted_d(two)
+    _, n_one, _ = oracle.grid_d(w)
+    assert n_two == 2.0 * n_one
