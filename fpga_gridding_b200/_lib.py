@@ -45,6 +45,7 @@ EXPORTED_SYMBOLS = (
     "oskar_b200_tune_table",
     "oskar_b200_measure_atomic_rate",
     "oskar_b200_grid_f_static",
+    "oskar_b200_grid_f_static_status",
     "oskar_b200_server_create",
     "oskar_b200_server_submit",
     "oskar_b200_server_poll",
@@ -54,6 +55,7 @@ EXPORTED_SYMBOLS = (
     "oskar_b200_server_free",
     "oskar_b200_selftest_bounded_wait",
     "oskar_b200_testing_fail_allocation",
+    "oskar_b200_testing_set_static_status",
     "oskar_b200_build_info",
 )
 
@@ -208,6 +210,10 @@ def load():
         _SZ, _P, C.c_int, C.c_int, _P, _SZ, _P, _P, _P, _P, C.c_float,
         C.c_float, C.c_int, _P, _P, _P, _P]
     lib.oskar_b200_grid_f_static.restype = C.c_int
+    lib.oskar_b200_grid_f_static_status.argtypes = [_P, C.POINTER(C.c_int)]
+    lib.oskar_b200_grid_f_static_status.restype = C.c_int
+    lib.oskar_b200_testing_set_static_status.argtypes = [C.c_ulonglong, _P]
+    lib.oskar_b200_testing_set_static_status.restype = C.c_int
     lib.oskar_b200_testing_fail_allocation.argtypes = [C.c_longlong]
     lib.oskar_b200_testing_fail_allocation.restype = C.c_int
     lib.oskar_b200_selftest_bounded_wait.argtypes = [_P, C.c_uint,

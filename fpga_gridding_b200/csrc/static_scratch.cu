@@ -70,7 +70,9 @@ int scratch_address(int device, unsigned char** out)
     return OSKAR_B200_OK;
 }
 
-// Bump allocator over the scratch array (256-byte aligned regions).
+// Bump allocator over the scratch array (256-byte aligned regions).  The
+// first region is always the counters (CNT_COUNT words), so the status word
+// sits at a fixed place whatever the size of the job that carved the rest.
 struct Carver
 {
     unsigned char* base;
@@ -249,6 +251,52 @@ extern "C" int oskar_b200_grid_f_static(
     int ctas = 0;
     B200_S(launch_grid(ga, 0, OSKAR_B200_KERNEL_NATIVE, max_block, false,
                        false, num_sms, s, &ctas));
-#undef B200_S
     return OSKAR_B200_OK;
 }
+
+namespace {
+
+// Device address of the status word of the static counters.
+int static_status_word(unsigned long long** word)
+{
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) return OSKAR_B200_ERR_NO_DEVICE;
+    unsigned char* base = nullptr;
+    const int st = scratch_address(device, &base);
+    if (st) return st;
+    *word = reinterpret_cast<unsigned long long*>(base) + CNT_STATUS;
+    return OSKAR_B200_OK;
+}
+
+}  // namespace
+
+extern "C" int oskar_b200_grid_f_static_status(void* stream, int* status)
+{
+    if (!status) return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    unsigned long long* word = nullptr;
+    const int st = static_status_word(&word);
+    if (st) return st;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    unsigned long long bits = 0;
+    B200_S(cudaMemcpyAsync(&bits, word, sizeof(bits), cudaMemcpyDeviceToHost,
+                           s));
+    B200_S(cudaStreamSynchronize(s));
+    *status = bits == 0 ? OSKAR_B200_OK
+              : (bits & DEV_ERR_TIMEOUT) ? OSKAR_B200_ERR_TIMEOUT
+                                         : OSKAR_B200_ERR_DEVICE_CHECK;
+    return OSKAR_B200_OK;
+}
+
+extern "C" int oskar_b200_testing_set_static_status(unsigned long long bits,
+                                                    void* stream)
+{
+    unsigned long long* word = nullptr;
+    const int st = static_status_word(&word);
+    if (st) return st;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // From pageable memory: the copy has staged `bits` when this returns.
+    B200_S(cudaMemcpyAsync(word, &bits, sizeof(bits), cudaMemcpyHostToDevice,
+                           s));
+    return OSKAR_B200_OK;
+}
+#undef B200_S

@@ -455,13 +455,32 @@ OSKAR_B200_EXPORT int oskar_b200_measure_atomic_rate(oskar_B200Workspace* ws,
  * current), so make that first call outside any stream capture.  Every call
  * shares the array: calls whose device work can overlap (other streams,
  * other threads) race and must be serialised by the caller.  Asynchronous on
- * `stream` (NULL: the legacy default stream). */
+ * `stream` (NULL: the legacy default stream).  The return value covers the
+ * arguments and the enqueueing only; the kernels' own checks land in a
+ * status word inside the static array, read with
+ * oskar_b200_grid_f_static_status.  The library holds the array's address
+ * for the life of the process, so resetting the device (cudaDeviceReset)
+ * after the first call is not supported. */
 OSKAR_B200_EXPORT int oskar_b200_grid_f_static(size_t num_w_planes,
         const int* support, int oversample, int conv_size_half,
         const float* conv_func, size_t num_points, const float* uu,
         const float* vv, const float* ww, const float* vis,
         float cell_size_rad, float w_scale, int grid_size, float* grid,
         unsigned long long* d_num_skipped, double* d_norm, void* stream);
+
+/* Device-side outcome of the latest oskar_b200_grid_f_static call on the
+ * current device (no counterpart in the reference, whose CPU gridder cannot
+ * fail).  Each call clears the status word in the static array before its
+ * kernels run, and the kernels' bounds checks and bounded waits OR their
+ * findings into it.  This copies the word back on `stream` (the stream of
+ * the call, or one ordered after it), waits for that copy, and writes
+ * *status: OSKAR_B200_OK, OSKAR_B200_ERR_DEVICE_CHECK (a bounds check
+ * fired; the grid may be incomplete) or OSKAR_B200_ERR_TIMEOUT (a bounded
+ * wait expired).  Allocates nothing.  A later call overwrites the word, so
+ * read it before the next call; a call refused by its return value runs no
+ * kernels and leaves the word as it was. */
+OSKAR_B200_EXPORT int oskar_b200_grid_f_static_status(void* stream,
+        int* status);
 
 /* ---------------------------------------------------------------------- */
 /* 3. Serving                                                             */
@@ -542,6 +561,15 @@ OSKAR_B200_EXPORT int oskar_b200_selftest_bounded_wait(
  * OSKAR_B200_ERR_OUT_OF_MEMORY and leaves the caller's outputs untouched
  * without exhausting a shared GPU.  Process-wide; not for production use. */
 OSKAR_B200_EXPORT int oskar_b200_testing_fail_allocation(long long after);
+
+/* Testing aid for oskar_b200_grid_f_static_status (no counterpart in the
+ * reference): enqueues on `stream` a write of `bits` (device check bits:
+ * 1 grid index, 2 slab index, 4 wait timeout, 8 task bounds) into the
+ * static array's status word on the current device, as a kernel whose check
+ * fired would.  Lets a test see the reader report a failure, and the next
+ * gridding call clear it, without provoking a fault on the GPU. */
+OSKAR_B200_EXPORT int oskar_b200_testing_set_static_status(
+        unsigned long long bits, void* stream);
 
 /* Library build description (arch, version). */
 OSKAR_B200_EXPORT const char* oskar_b200_build_info(void);
