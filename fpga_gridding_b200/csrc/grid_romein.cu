@@ -4,10 +4,12 @@
 // a w-plane (hence a support S and footprint width W = 2S+1) and a coarse
 // grid tile.  A persistent CTA pulls tasks from a device work queue.  For a
 // task it
-//   1. stages the plane's re-laid kernel slab into shared memory with one
-//      TMA bulk copy (cp.async.bulk + mbarrier), skipped when the previous
-//      task of this CTA used the same plane,
-//   2. turns each visibility into a small tap record in shared memory,
+//   1. orders the task's visibilities by cell (and kernel row offset) and
+//      turns each into a small tap record in shared memory, merging records
+//      whose taps are identical,
+//   2. reads kernel values through L1 (default) or, with staging on, copies
+//      the W-row block of each kernel row offset into shared memory with
+//      TMA bulk copies (cp.async.bulk + mbarrier) before that offset's run,
 //   3. lets each thread own "classes" (a, b) in [0, W)^2: for every
 //      visibility, the class's grid point is the unique footprint cell
 //      (u, v) with u = a (mod W) and v = b (mod W).  Consecutive (spatially

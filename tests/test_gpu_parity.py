@@ -290,6 +290,39 @@ def test_launch_variants_fp64(ws, oracle, small, staging, cpt):
     assert abs(n2 - n1) <= TOL_D * abs(n1)
 
 
+def _weighted(w, seed=4):
+    """The job with weights U(0.25, 4) instead of ones."""
+    out = dict(w)
+    out["weight"] = np.random.default_rng(seed).uniform(0.25, 4.0,
+                                                        len(w["uu"]))
+    return out
+
+
+def test_weighted_gridding_fp64_matches_oracle(ws, oracle, small):
+    """apply_weight = 1: each visibility scaled by its weight and the norm
+    by tap sum x weight (the reference tiled CUDA gridder's weighting,
+    restated in the oracle)."""
+    w = _weighted(small)
+    s1, n1, g1 = oracle.grid_weighted_d(w)
+    s2, n2, g2, st = _grid_ext(ws, w, False, apply_weight=1)
+    assert s2 == s1 and st.status == 0
+    assert oracle.rel_rms(g2, g1) <= TOL_D
+    assert abs(n2 - n1) <= TOL_D * abs(n1)
+    # the weights really act: the unweighted grid is far from this one
+    _, _, g0 = oracle.grid_d(small, threads=8)
+    assert oracle.rel_rms(g0, g1) > 0.1
+
+
+@pytest.mark.parametrize("staging", [0, 1])
+def test_weighted_gridding_fp32_matches_oracle(ws, oracle, small, staging):
+    w = _weighted(small)
+    s1, n1, g1 = oracle.grid_weighted_d(promote(w))
+    s2, n2, g2, st = _grid_ext(ws, w, True, apply_weight=1, staging=staging)
+    assert s2 == s1 and st.status == 0
+    assert oracle.rel_rms(g2, g1) <= TOL_F
+    assert abs(n2 - n1) <= TOL_D * abs(n1)
+
+
 def test_stats_count_grid_updates(ws, oracle, small):
     _, _, _, st = _grid_ext(ws, small, True)
     assert st.grid_updates == oracle.count_taps(small)
