@@ -24,6 +24,7 @@ from __future__ import annotations
 import argparse
 import datetime
 import json
+import math
 import os
 import re
 import statistics
@@ -583,15 +584,38 @@ def run_batch128(args, world, rank, local):
         cb.close()
     del jobs32
 
-    # (c) one batch, FP16 kernels + compensated accumulation, graph-captured
+    # (c) compensation on the heavily hit central cells only: the radius
+    # (Chebyshev distance from the grid centre, in cells, tested per task)
+    # holding half of all channels' visibilities, where the uv density and
+    # hence each cell's running sum are largest.
+    radius = central_radius(chans, 0.5)
+    comp_c = fg.options(accum_mode=_lib.ACCUM_COMPENSATED,
+                        compensate_radius=radius)
+    cubes32, jobs32 = make_jobs(_lib.KERNEL_NATIVE)
+    gc = graph_of(jobs32, comp_c)
+    batch32c_ms = timed(replay_on_s(gc))
+    del gc
+    err32c = {}
+    if rank == 0 and not args.no_cpu_baseline:
+        err32c = audit_batch(chans, cubes32, ws, comp_c)
+    for cb in cubes32:
+        cb.close()
+    del jobs32
+
+    # (d) one batch, FP16 kernels + compensated accumulation (whole grid,
+    # then central cells), graph-captured
     cubes16, jobs16 = make_jobs(_lib.KERNEL_F16)
     comp = fg.options(accum_mode=_lib.ACCUM_COMPENSATED)
     g16 = graph_of(jobs16, comp)
     batch16_ms = timed(replay_on_s(g16))
     del g16
-    err16 = {}
+    g16c = graph_of(jobs16, comp_c)
+    batch16c_ms = timed(replay_on_s(g16c))
+    del g16c
+    err16, err16c = {}, {}
     if rank == 0 and not args.no_cpu_baseline:
         err16 = audit_batch(chans, cubes16, ws, comp)
+        err16c = audit_batch(chans, cubes16, ws, comp_c)
     for cb in cubes16:
         cb.close()
     value = n_total * world / (batch32_ms * 1e-3) / 1e9
@@ -614,13 +638,38 @@ def run_batch128(args, world, rank, local):
                          "grid": round(st.grid_ms, 3)},
             "gpu_launches": st.kernel_launches * args.steps,
             "rel_err_vs_fp64": err,
+            "compensate_radius_cells": radius,
+            "f32_compensated_central_batch": {
+                "ms_per_step": round(batch32c_ms, 3),
+                "value": round(n_total * world / (batch32c_ms * 1e-3) / 1e9, 4),
+                "speedup_vs_sequential_plain_fp32": round(seq_ms / batch32c_ms, 3),
+                "rel_err_vs_fp64": err32c},
             "f16_compensated_batch": {
                 "ms_per_step": round(batch16_ms, 3),
                 "value": round(n_total * world / (batch16_ms * 1e-3) / 1e9, 4),
+                "speedup_vs_sequential_plain_fp32": round(seq_ms / batch16_ms, 3),
                 "rel_err_vs_fp64": err16,
                 "note": "FP16 kernel cubes quantise the kernel values to "
-                        "about 1e-4 relative, above the 1e-5 bar"},
+                        "about 1e-4 relative, above the 1e-5 bar: a "
+                        "1e-4 mode"},
+            "f16_compensated_central_batch": {
+                "ms_per_step": round(batch16c_ms, 3),
+                "value": round(n_total * world / (batch16c_ms * 1e-3) / 1e9, 4),
+                "speedup_vs_sequential_plain_fp32": round(seq_ms / batch16c_ms, 3),
+                "rel_err_vs_fp64": err16c},
             "clocks": clk}
+
+
+def central_radius(chans, frac):
+    """Chebyshev distance from the grid centre, in cells, within which
+    `frac` of all channels' visibilities lie."""
+    d = []
+    for c in chans:
+        sc = c.grid_size * float(np.float32(c.cell_size_rad))
+        d.append(torch.maximum(c.uu.abs(), c.vv.abs()).float() * sc)
+    d = torch.cat(d)
+    k = max(1, int(frac * d.numel()))
+    return int(math.ceil(float(torch.kthvalue(d, k).values))) + 1
 
 
 def audit_batch(chans, cubes, ws, opts, m=100000):
@@ -661,7 +710,7 @@ def audit_batch(chans, cubes, ws, opts, m=100000):
 
 SERVING_DESC = ("serving: 2000 jobs, visibilities log-uniform in 1e4-5e7, "
                 "grids {512,1024,2048,4096,8192}^2 FP32, 8-256 w-planes, "
-                "support 3-32, FP16 kernel cubes (20% shared), seeded Poisson "
+                "support 3-32, {kt} kernel cubes (20% shared), seeded Poisson "
                 "arrivals at 70% of measured capacity, 150 GB HBM budget")
 
 
@@ -678,10 +727,12 @@ def run_serving(args, world, rank, local):
                                          device="cuda")
     ws = fg.Workspace(local)
     cubes = {}
+    f16 = args.serving_kernel == "f16"
     for key, (sup, csh) in specs.items():
         cube = W.analytic_kernel_cube(sup, 4, csh, device="cuda").float()
         cubes[key] = fg.Cube(ws, sup, 4, csh, cube, data_is_double=False,
-                             kernel_type=_lib.KERNEL_F16)
+                             kernel_type=_lib.KERNEL_F16 if f16
+                             else _lib.KERNEL_NATIVE)
         del cube
     torch.cuda.synchronize()
     srv = Server(local, budget_bytes=150 << 30, slots=args.serving_slots,
@@ -817,8 +868,10 @@ def run_serving(args, world, rank, local):
             "unit": UNIT, "n_gpus": world, "steps": num_jobs, "warmup": 16,
             "ms_per_step": round(1e3 * span / num_jobs, 3),
             "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f16 kernels, f32", "data": DATA_DESC,
-            "config": {"workload": SERVING_DESC, "jobs": num_jobs,
+            "vs_baseline": None,
+            "dtype": "f16 kernels, f32" if f16 else "f32", "data": DATA_DESC,
+            "config": {"workload": SERVING_DESC.format(
+                           kt="FP16" if f16 else "FP32"), "jobs": num_jobs,
                        "points": points, "slots": args.serving_slots,
                        "max_batch": args.serving_batch},
             "capacity_jobs_per_s": capacity,
@@ -1412,6 +1465,11 @@ def main():
                     help="concurrent batches the server keeps on the GPU")
     ap.add_argument("--serving-batch", type=int, default=32,
                     help="most jobs the server puts in one batch")
+    ap.add_argument("--serving-kernel", choices=("f32", "f16"),
+                    default="f32",
+                    help="kernel-cube storage of the serving jobs (FP16 "
+                         "quantises kernel values to ~1e-4 relative, above "
+                         "the 1e-5 bar)")
     ap.add_argument("--stations", type=int, default=512,
                     help="stations of the job (512 = the benchmark job; "
                          "fewer = a smaller profiling case)")

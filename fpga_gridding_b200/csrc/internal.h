@@ -264,9 +264,19 @@ struct HostJob
 // one sort and one persistent gridding launch.  degrid: the same placement
 // and sort, then the adjoint (degrid.cu): each job's `grid` is read and its
 // `vis` written.
+// time_slices > 1 (at most kMaxBands; not with bands or degrid): the
+// gridding kernel runs as that many launches over contiguous ranges of the
+// task list, so that the device can schedule other streams' work between
+// them (the server's large batches).
 int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
               int num_jobs, const HostJob* jobs, cudaStream_t st,
-              bool degrid = false, BandPlan* bands = nullptr);
+              bool degrid = false, BandPlan* bands = nullptr,
+              int time_slices = 1);
+// first[0..k_slices] = the bounds of k_slices equal ranges of the task
+// list; queues[0..k_slices) = 0.
+cudaError_t launch_slice_bounds(const unsigned long long* counters,
+                                int k_slices, uint32_t* first,
+                                unsigned long long* queues, cudaStream_t st);
 
 // ---- degrid.cu ------------------------------------------------------------
 cudaError_t launch_degrid(const uint32_t* order, const uint32_t* sorted_keys,

@@ -81,8 +81,11 @@ double coord_scale_of(double frequency_hz)
 
 int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
               int num_jobs, const HostJob* jobs, cudaStream_t st,
-              bool degrid, BandPlan* bands)
+              bool degrid, BandPlan* bands, int time_slices)
 {
+    if (time_slices < 1 || time_slices > kMaxBands ||
+        (time_slices > 1 && (bands || degrid)))
+        return OSKAR_B200_ERR_INVALID_ARGUMENT;
     // (the error grid is folded in after the last band: not band-ordered)
     if (bands && (num_jobs != 1 || degrid || !bands->events ||
                   opt->accum_mode == OSKAR_B200_ACCUM_COMPENSATED))
@@ -131,6 +134,7 @@ int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
         // (the layout already holds: at most 16 coarse tiles per axis)
         B200_TRY(ws->bands.ensure(256));
     }
+    if (time_slices > 1) B200_TRY(ws->bands.ensure(256));
     // Every band event is recorded on every successful path.
     auto record_bands = [&]() -> cudaError_t {
         if (!bands) return cudaSuccess;
@@ -399,6 +403,28 @@ int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
             launches += 1;
         }
     }
+    else if (time_slices > 1)
+    {
+        // The task list in time_slices contiguous ranges, one launch each:
+        // the persistent CTAs of one launch retire when its range is done,
+        // so work queued on other streams (of higher priority) gets SMs
+        // between slices instead of waiting for the whole job.
+        uint32_t* first = static_cast<uint32_t*>(ws->bands.ptr);
+        unsigned long long* queues = reinterpret_cast<unsigned long long*>(
+            static_cast<unsigned char*>(ws->bands.ptr) + 128);
+        B200_TRY(launch_slice_bounds(counters, time_slices, first, queues,
+                                     st));
+        launches += 1;
+        B200_TRY(mark(3));
+        for (int k = 0; k < time_slices; ++k)
+        {
+            ga.range = first + k;
+            ga.queue = queues + k;
+            B200_TRY(launch_grid(ga, dbl, c0->kernel_type, max_block, staged,
+                                 comp, ws->num_sms, st, &ctas));
+            launches += 1;
+        }
+    }
     else
     {
         B200_TRY(mark(3));
@@ -525,7 +551,30 @@ __global__ void status_or_kernel(const unsigned long long* counters,
     if (counters[CNT_STATUS]) *acc |= counters[CNT_STATUS];
 }
 
+// first[k] = floor(T * k / K) for k in [0, K], T the task count of the
+// gridding launch; the K work-queue heads are zeroed.
+__global__ void slice_bounds_kernel(const unsigned long long* counters,
+                                    int k_slices, uint32_t* first,
+                                    unsigned long long* queues)
+{
+    const unsigned long long t = counters[CNT_TASKS];
+    for (int k = threadIdx.x; k <= k_slices; k += blockDim.x)
+    {
+        first[k] = (uint32_t)(t * (unsigned long long)k /
+                              (unsigned long long)k_slices);
+        if (k < k_slices) queues[k] = 0;
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_slice_bounds(const unsigned long long* counters,
+                                int k_slices, uint32_t* first,
+                                unsigned long long* queues, cudaStream_t st)
+{
+    slice_bounds_kernel<<<1, 32, 0, st>>>(counters, k_slices, first, queues);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_add(void* dst, const void* src, size_t n, int is_double,
                        int num_sms, cudaStream_t st)

@@ -1,16 +1,30 @@
 // Resident gridding server: continuous batching of independent jobs on one
 // device.
 //
-// A server thread owns `num_slots` slots, each a workspace with its own
-// stream.  Submitted jobs wait in arrival order.  Whenever a slot is free the
-// thread takes the head job plus the following queued jobs that fit in the
-// same launch (same precision and kernel storage, at most max_batch jobs and
+// A server thread owns `num_slots` slots, each a workspace with two streams
+// (the workspace's own, and one of the device's highest priority).
+// Submitted jobs wait in arrival order.  Whenever a slot is free the thread
+// takes the head job plus the following queued jobs that fit in the same
+// launch (same precision and kernel storage, at most max_batch jobs and
 // kBatchPoints visibilities) and that fit the HBM budget, allocates and
 // zeroes their output grids, and enqueues one batched gridding call
-// (run_batch) on the slot's stream.  Slots run concurrently, so jobs that
-// arrive while others are on the device start as soon as a slot and memory
-// are free.  Completion is detected by polling a CUDA event per slot; the
-// job's skip count, norm and status are copied back through pinned memory.
+// (run_batch).  Slots run concurrently, so jobs that arrive while others are
+// on the device start as soon as a slot and memory are free.  Completion is
+// detected by polling a CUDA event per slot; the job's skip count, norm and
+// status are copied back through pinned memory.
+//
+// Large jobs must not hold up small ones.  A persistent gridding kernel
+// keeps every SM until its task queue is empty, and a running CTA is never
+// preempted, so three rules keep latency bounded under mixed sizes:
+//   * a batch of at most kSmallPoints visibilities runs on the slot's
+//     high-priority stream;
+//   * a larger batch grids in time slices (about kSlicePoints visibilities
+//     each, at most kMaxBands): its CTAs retire at each slice boundary and
+//     the SMs go to waiting high-priority work first;
+//   * with three or more slots the last slot takes small jobs only (the
+//     first small jobs in the queue, passing large ones), so a small job
+//     never waits for a slot while large jobs occupy the others.
+#include <algorithm>
 #include <cmath>
 #include <chrono>
 #include <condition_variable>
@@ -31,6 +45,8 @@ using namespace b200;
 namespace {
 
 constexpr size_t kBatchPoints = 8u << 20;   // visibilities per merged launch
+constexpr size_t kSmallPoints = 2u << 20;   // small: high-priority stream
+constexpr size_t kSlicePoints = 4u << 20;   // visibilities per time slice
 
 struct Pending
 {
@@ -48,6 +64,8 @@ struct Running
 struct Slot
 {
     oskar_B200Workspace* ws = nullptr;
+    cudaStream_t hi = nullptr;  // highest-priority stream (small batches)
+    bool small_only = false;    // reserved for small jobs
     bool busy = false;
     cudaEvent_t done = nullptr;
     DeviceBuffer outs;          // per job: skipped (u64), norm (f64)
@@ -181,29 +199,39 @@ struct oskar_B200Server
         for (Slot& s : slots)
         {
             if (s.busy || queue.empty()) continue;
-            const oskar_B200Cube* c0 = queue.front().req.cube;
-            const bool dbl = c0->data_is_double != 0;
-            // Take the head and the following compatible jobs that fit.
+            // The batch: a general slot takes the head and the following
+            // compatible jobs that fit; a small-only slot takes the first
+            // small job and the following compatible small ones, passing
+            // large ones.
+            std::vector<size_t> pick;
+            const oskar_B200Cube* c0 = nullptr;
             size_t n = 0, gbytes = 0;
-            size_t count = 0;
             const size_t have = oskar_b200_workspace_bytes(s.ws);
-            for (const Pending& p : queue)
+            for (size_t qi = 0; qi < queue.size(); ++qi)
             {
-                if ((int)count >= max_batch) break;
-                if (p.req.cube->data_is_double != c0->data_is_double ||
-                    p.req.cube->kernel_type != c0->kernel_type)
+                const Pending& p = queue[qi];
+                if (s.small_only && p.req.num_points > kSmallPoints) continue;
+                if ((int)pick.size() >= max_batch) break;
+                if (c0 && (p.req.cube->data_is_double != c0->data_is_double ||
+                           p.req.cube->kernel_type != c0->kernel_type))
+                {
+                    if (s.small_only) continue;
                     break;
-                if (count > 0 && n + p.req.num_points > kBatchPoints) break;
+                }
+                if (!pick.empty() && n + p.req.num_points > kBatchPoints) break;
+                const bool dbl = p.req.cube->data_is_double != 0;
                 const size_t ws_need = workspace_need(n + p.req.num_points, dbl);
                 const size_t grow = ws_need > have ? ws_need - have : 0;
                 trim_pool(grow + gbytes + p.grid_bytes);
                 if (in_use() + grow + gbytes + p.grid_bytes > budget) break;
+                if (!c0) c0 = p.req.cube;
                 n += p.req.num_points;
                 gbytes += p.grid_bytes;
-                ++count;
+                pick.push_back(qi);
             }
-            if (count == 0)
+            if (pick.empty())
             {
+                if (s.small_only) continue;
                 // The head does not fit now; if nothing runs it never will.
                 bool any_busy = false;
                 for (const Slot& o : slots) any_busy |= o.busy;
@@ -214,19 +242,34 @@ struct oskar_B200Server
                 }
                 break;
             }
+            // Take the picked jobs out of the queue, keeping the order of
+            // the others.
+            std::vector<Pending> batch;
+            batch.reserve(pick.size());
+            for (size_t k = pick.size(); k-- > 0;)
+            {
+                batch.push_back(queue[pick[k]]);
+                queue.erase(queue.begin() + (std::ptrdiff_t)pick[k]);
+            }
+            std::reverse(batch.begin(), batch.end());
+            const size_t count = batch.size();
+            const bool small = n <= kSmallPoints;
+            const int slices = small ? 1 : (int)std::min<size_t>(
+                (size_t)kMaxBands, (n + kSlicePoints - 1) / kSlicePoints);
             std::vector<HostJob> jobs(count);
             s.jobs.clear();
-            cudaStream_t st = s.ws->stream;
+            cudaStream_t st = small ? s.hi : s.ws->stream;
             bool ok = true;
             for (size_t i = 0; i < count; ++i)
             {
-                Pending p = queue.front();
-                queue.pop_front();
+                Pending p = batch[i];
                 void* g = take_grid(p.grid_bytes);
                 if (!g || cudaMemsetAsync(g, 0, p.grid_bytes, st) != cudaSuccess)
                 {
+                    // Put this job and the rest back at the head.
                     ok = false;
-                    queue.push_front(p);
+                    for (size_t r = count; r-- > i;)
+                        queue.push_front(batch[r]);
                     break;
                 }
                 live[p.req.tag] = std::make_pair(g, p.grid_bytes);
@@ -243,7 +286,8 @@ struct oskar_B200Server
             if (!ok && s.jobs.empty()) break;
             jobs.resize(s.jobs.size());
             cudaMemsetAsync(s.outs.ptr, 0, 16 * jobs.size(), st);
-            int rs = run_batch(s.ws, &opt, (int)jobs.size(), jobs.data(), st);
+            int rs = run_batch(s.ws, &opt, (int)jobs.size(), jobs.data(), st,
+                               false, nullptr, slices);
             if (rs == OSKAR_B200_OK)
             {
                 cudaMemcpyAsync(s.h_outs, s.outs.ptr, 16 * jobs.size(),
@@ -334,11 +378,20 @@ int oskar_b200_server_create(int device, size_t hbm_budget_bytes,
     int prev = 0;
     cudaGetDevice(&prev);
     int st = OSKAR_B200_OK;
+    int least_prio = 0, greatest_prio = 0;
     for (Slot& sl : s->slots)
     {
         st = oskar_b200_workspace_create(device, &sl.ws);
         if (st) break;
         cudaSetDevice(device);
+        cudaDeviceGetStreamPriorityRange(&least_prio, &greatest_prio);
+        if (cudaStreamCreateWithPriority(&sl.hi, cudaStreamNonBlocking,
+                                         greatest_prio) != cudaSuccess)
+        {
+            cudaGetLastError();
+            st = OSKAR_B200_ERR_CUDA;
+            break;
+        }
         if (cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) !=
                 cudaSuccess ||
             sl.outs.ensure(16 * (size_t)max_batch_jobs) != cudaSuccess ||
@@ -355,6 +408,7 @@ int oskar_b200_server_create(int device, size_t hbm_budget_bytes,
         for (Slot& sl : s->slots)
         {
             if (sl.done) cudaEventDestroy(sl.done);
+            if (sl.hi) cudaStreamDestroy(sl.hi);
             if (sl.h_outs) cudaFreeHost(sl.h_outs);
             sl.outs.release();
             if (sl.ws) oskar_b200_workspace_free(sl.ws);
@@ -362,6 +416,7 @@ int oskar_b200_server_create(int device, size_t hbm_budget_bytes,
         delete s;
         return st;
     }
+    if (num_slots >= 3) s->slots.back().small_only = true;
     s->t0 = std::chrono::steady_clock::now();
     s->thread = std::thread([s] { s->loop(); });
     *server = s;
@@ -455,6 +510,7 @@ int oskar_b200_server_free(oskar_B200Server* s)
     for (Slot& sl : s->slots)
     {
         if (sl.done) cudaEventDestroy(sl.done);
+        if (sl.hi) cudaStreamDestroy(sl.hi);
         if (sl.h_outs) cudaFreeHost(sl.h_outs);
         sl.outs.release();
         oskar_b200_workspace_free(sl.ws);

@@ -490,7 +490,12 @@ OSKAR_B200_EXPORT int oskar_b200_grid_f_static_status(void* stream,
  * submitted jobs in arrival order as slots and memory free up: each of
  * `num_slots` slots owns a workspace and a stream, so admitted jobs run
  * concurrently on the device; queued jobs that fit together are merged into
- * one batched launch (continuous batching).  The server owns each job's
+ * one batched launch (continuous batching).  Large jobs do not hold up
+ * small ones: batches of up to 2^21 visibilities run on a stream of the
+ * device's highest priority, larger batches grid in time slices of about
+ * 2^22 visibilities whose SMs go to waiting high-priority work first, and
+ * with three or more slots the last slot takes only such small jobs
+ * (passing large ones in the queue).  The server owns each job's
  * output grid, allocated (zeroed) at admission; the HBM budget covers the
  * slots' workspaces and the live output grids, and a job waits until it
  * fits.  Cubes and input visibilities stay the caller's (device memory). */

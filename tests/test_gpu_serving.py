@@ -126,3 +126,48 @@ def test_budget_is_respected_and_impossible_job_rejected():
     for c in cubes:
         c.close()
     ws.close()
+
+
+def test_time_sliced_large_job_and_reserved_small_slot():
+    """A job of about 8.9 million visibilities (above the server's
+    small-batch and slice sizes, so its gridding runs as several
+    time-sliced launches) submitted with small jobs, which the reserved
+    small-job slot takes past it on the high-priority stream: every result
+    equals the same job gridded alone."""
+    big = W.plain_small(seed=21, num_stations=128, num_times=1100,
+                        grid_size=1024, num_w_planes=16)
+    assert big.num_points > 8_000_000
+    small = _jobs()[:3]
+    b32 = big.to(dtype=torch.float32, device="cuda")
+    jobs = [dict(wl=big, uu=b32.uu, vv=b32.vv, ww=b32.ww, vis=b32.vis,
+                 weight=b32.weight, cell=float(np.float32(big.cell_size_rad)),
+                 wsc=float(np.float32(big.w_scale)), g=big.grid_size)] + small
+    ws = fg.Workspace(0)
+    cubes = [fg.Cube(ws, j["wl"].support, j["wl"].oversample,
+                     j["wl"].conv_size_half,
+                     np.asarray(j["wl"].conv_func, np.float32),
+                     data_is_double=False) for j in jobs]
+    srv = Server(0, budget_bytes=16 << 30, slots=3, max_batch=4)
+    for t, (j, c) in enumerate(zip(jobs, cubes)):
+        srv.submit(t, c, j["uu"], j["vv"], j["ww"], j["vis"], j["weight"],
+                   j["cell"], j["wsc"], j["g"])
+    done = _collect(srv, len(jobs))
+    for t, (j, c) in enumerate(zip(jobs, cubes)):
+        comp = done[t]
+        assert comp["status"] == 0
+        mix = srv.grid(comp).cpu().numpy()
+        alone = torch.zeros(2 * j["g"] ** 2, device="cuda")
+        skip = torch.zeros(1, dtype=torch.int64, device="cuda")
+        norm = torch.zeros(1, dtype=torch.float64, device="cuda")
+        fg.grid_device(ws, c, j["uu"], j["vv"], j["ww"], j["vis"],
+                       j["weight"], j["cell"], j["wsc"], j["g"], alone, skip,
+                       norm)
+        torch.cuda.synchronize()
+        assert comp["num_skipped"] == int(skip.item())
+        assert abs(comp["norm"] - norm.item()) <= 1e-13 * abs(norm.item())
+        assert rel_rms(mix, alone.cpu().numpy()) <= 2e-6
+        srv.release(t)
+    srv.close()
+    for c in cubes:
+        c.close()
+    ws.close()
