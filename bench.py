@@ -285,6 +285,8 @@ def run_b200(args, world, rank, local):
         smp = wl.subset(idx)
         tuned = ws.autotune(cube, smp.uu, smp.vv, smp.ww, smp.vis, cell, wsc,
                             g, grid).tolist()
+        tuned_launch = dict(zip(("tile_shift", "staging",
+                                 "compensate_radius"), ws.tune_launch()))
         grid.zero_()
 
     def step():
@@ -393,6 +395,7 @@ def run_b200(args, world, rank, local):
     if tuned is not None:
         sup = [int(x) for x in np.unique(wl.support)]
         out["autotuned_classes_per_thread"] = {s: tuned[s] for s in sup}
+        out["autotuned_launch"] = tuned_launch
     if rank == 0 and world == 1 and not args.no_cpu_baseline and \
             args.stations == 512:
         out["cpu_baseline"] = run_cpu_baseline(args, wl)

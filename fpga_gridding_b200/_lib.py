@@ -43,6 +43,7 @@ EXPORTED_SYMBOLS = (
     "oskar_b200_set_stage_timing",
     "oskar_b200_autotune",
     "oskar_b200_tune_table",
+    "oskar_b200_tune_launch",
     "oskar_b200_measure_atomic_rate",
     "oskar_b200_grid_f_static",
     "oskar_b200_grid_f_static_status",
@@ -83,7 +84,7 @@ class Options(C.Structure):
     _fields_ = [("coord_mode", C.c_int), ("kernel_type", C.c_int),
                 ("accum_mode", C.c_int), ("apply_weight", C.c_int),
                 ("classes_per_thread", C.c_int), ("staging", C.c_int),
-                ("compensate_radius", C.c_int), ("reserved0", C.c_int),
+                ("compensate_radius", C.c_int), ("tile_shift", C.c_int),
                 ("frequency_hz", C.c_double), ("reserved", C.c_int * 6)]
 
 
@@ -202,6 +203,8 @@ def load():
         _P, _P, C.POINTER(Options), _SZ, _P, _P, _P, _P, C.c_double,
         C.c_double, C.c_int, _P, _P]
     lib.oskar_b200_tune_table.argtypes = [_P, _P, _P]
+    lib.oskar_b200_tune_launch.argtypes = [_P, _P, _P]
+    lib.oskar_b200_tune_launch.restype = C.c_int
     lib.oskar_b200_measure_atomic_rate.argtypes = [
         _P, _P, C.c_int, C.c_int, C.POINTER(C.c_double)]
     lib.oskar_b200_grid_batch.argtypes = [_P, C.POINTER(Options), C.c_int,

@@ -477,6 +477,9 @@ int check_options(const oskar_B200Options* opt, int data_is_double)
         return OSKAR_B200_ERR_UNSUPPORTED;
     if (opt->staging < 0 || opt->staging > 2)
         return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    if (opt->compensate_radius < -1 ||
+        (opt->tile_shift != 0 && (opt->tile_shift < 6 || opt->tile_shift > 15)))
+        return OSKAR_B200_ERR_INVALID_ARGUMENT;
     if (!(opt->frequency_hz >= 0.0) || !std::isfinite(opt->frequency_hz))
         return OSKAR_B200_ERR_INVALID_ARGUMENT;
     return OSKAR_B200_OK;
@@ -900,6 +903,29 @@ int oskar_b200_tune_table(oskar_B200Workspace* ws, const unsigned char* table,
             memcpy(current, ws->tune, sizeof(ws->tune));
         else
             default_tune_table(current);
+    }
+    return OSKAR_B200_OK;
+}
+
+int oskar_b200_tune_launch(oskar_B200Workspace* ws, const int* set,
+                           int* current)
+{
+    if (!ws) return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    if (set)
+    {
+        if ((set[0] != 0 && (set[0] < 6 || set[0] > 15)) ||
+            (set[1] != 1 && set[1] != 2) || set[2] < 0)
+            return OSKAR_B200_ERR_INVALID_ARGUMENT;
+        ws->tuned_tile_shift = set[0];
+        ws->tuned_staging = set[1];
+        ws->tuned_comp_radius = set[2];
+        ws->tuned_launch = 1;
+    }
+    if (current)
+    {
+        current[0] = ws->tuned_launch ? ws->tuned_tile_shift : 0;
+        current[1] = ws->tuned_launch ? ws->tuned_staging : 2;
+        current[2] = ws->tuned_launch ? ws->tuned_comp_radius : 0;
     }
     return OSKAR_B200_OK;
 }

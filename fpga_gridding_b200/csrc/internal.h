@@ -168,6 +168,12 @@ struct oskar_B200Workspace
     // classes-per-thread table measured by oskar_b200_autotune
     unsigned char tune[128] = {};
     int tuned = 0;
+    // launch shape picked by oskar_b200_autotune (or set): coarse tile
+    // shift (0: automatic), staging (1 shared, 2 L1), compensation radius
+    int tuned_launch = 0;
+    int tuned_tile_shift = 0;
+    int tuned_staging = 2;
+    int tuned_comp_radius = 0;
 };
 
 struct oskar_B200Cube
@@ -238,8 +244,10 @@ struct KeyLayout
 };
 // Layout for the largest grid and plane count of the batch; false if the
 // fields cannot fit 31 bits.
+// tile_shift > 0 sets the coarse tile side to 2^tile_shift cells (at least
+// 64, at most the grid); 0 picks grid_size / 16.
 bool make_key_layout(int grid_size, int num_planes, int num_jobs,
-                     KeyLayout* out);
+                     KeyLayout* out, int tile_shift = 0);
 
 // One job of a batch, host side.
 struct HostJob

@@ -120,7 +120,10 @@ int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
     if (n >= 0xffffffffull) return OSKAR_B200_ERR_INVALID_ARGUMENT;
     ws->last_points = n;
     KeyLayout kl;
-    if (!make_key_layout(max_grid, max_planes, num_jobs, &kl))
+    // Launch shape: the options', else the workspace's tuned one.
+    const int tile_shift = opt->tile_shift > 0 ? opt->tile_shift
+                           : ws->tuned_launch ? ws->tuned_tile_shift : 0;
+    if (!make_key_layout(max_grid, max_planes, num_jobs, &kl, tile_shift))
         return OSKAR_B200_ERR_UNSUPPORTED;
     if (bands)
     {
@@ -358,7 +361,8 @@ int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
     ga.task_job = static_cast<const uint32_t*>(ws->task_job.ptr);
     ga.jobs = d_jobs;
     ga.counters = counters;
-    ga.comp_radius = opt->compensate_radius;
+    ga.comp_radius = opt->compensate_radius >= 0 ? opt->compensate_radius
+                     : ws->tuned_launch ? ws->tuned_comp_radius : 0;
     // Counting the grid atomics costs an instruction per tap: only when the
     // caller asked for it (statistics level bit 1).
     ga.count_flushes = (ws->stage_timing & 2) ? 1 : 0;
@@ -373,7 +377,9 @@ int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
     // plain_large the L1 path is as fast as staging each row-offset run's
     // W-row block into shared memory (24.2 ms vs 24.8 ms with FP16 slabs,
     // 30.2 ms with FP32 slabs, whose blocks cap residency at 2 CTAs/SM).
-    const bool staged = opt->staging == 1;
+    const bool staged = opt->staging == 1 ||
+                        (opt->staging == 0 && !comp && ws->tuned_launch &&
+                         ws->tuned_staging == 1);
     if (staged && grid_smem_bytes(dbl, max_block, true) > ws->smem_optin)
         return OSKAR_B200_ERR_UNSUPPORTED;
     if (comp)

@@ -3,6 +3,8 @@
 // oskar_grid_wproj.c:70-101 computes it, the sort key, the skip counts, the
 // norms and the plane histograms; then, after the sort, the permutation into
 // sorted order and the gridding work list (tasks).
+#include <algorithm>
+
 #include "common.cuh"
 #include "internal.h"
 #include "prep.cuh"
@@ -15,14 +17,17 @@ namespace b200 {
 constexpr int kKeyBits = 32;
 
 bool make_key_layout(int grid_size, int num_planes, int num_jobs,
-                     KeyLayout* out)
+                     KeyLayout* out, int tile_shift)
 {
     KeyLayout k{};
     int gbits = 0;
     while ((1 << gbits) < grid_size) ++gbits;
     // Coarse tiles: at most 16 per axis and at least 64 cells wide, so the
-    // visibilities in flight at any time touch a few coarse tiles of grid.
+    // visibilities in flight at any time touch a few coarse tiles of grid
+    // (or the width asked for, within 64 cells and the grid).
     k.coarse_shift = gbits - 4 > 6 ? gbits - 4 : 6;
+    if (tile_shift > 0)
+        k.coarse_shift = std::max(6, std::min(tile_shift, std::max(gbits, 6)));
     const int ctiles = (grid_size + (1 << k.coarse_shift) - 1) >> k.coarse_shift;
     while ((1 << k.coarse_bits) < ctiles) ++k.coarse_bits;
     while ((1 << k.plane_bits) < num_planes) ++k.plane_bits;

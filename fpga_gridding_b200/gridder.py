@@ -194,9 +194,12 @@ class Workspace:
     def autotune(self, cube, uu, vv, ww, vis, cell_size_rad: float,
                  w_scale: float, grid_size: int, grid,
                  opts: Options | None = None) -> np.ndarray:
-        """Measures the fastest classes-per-thread per support on a sample
-        job (device tensors; `grid` is scratch) and keeps it for later
-        calls on this workspace.  Returns the table (index = support)."""
+        """Measures the fastest classes-per-thread per support, then the
+        tile width and kernel-value path, and (with compensated accumulation
+        in `opts`) the compensation radius on a sample job (device tensors;
+        `grid` is scratch), and keeps them for later calls on this
+        workspace.  Returns the classes-per-thread table (index = support);
+        tune_launch() reads the rest."""
         table = np.zeros(128, np.uint8)
         check(self._lib.oskar_b200_autotune(
             self.handle, cube.handle,
@@ -217,6 +220,18 @@ class Workspace:
             self.handle, t.ctypes.data_as(C.c_void_p) if t is not None
             else None, cur.ctypes.data_as(C.c_void_p)), "tune_table")
         return cur
+
+    def tune_launch(self, shape=None) -> tuple:
+        """Sets the launch shape (tile_shift, staging, compensate_radius)
+        that calls leaving these to the workspace use, if given; returns the
+        shape in use."""
+        cur = (C.c_int * 3)()
+        arr = None
+        if shape is not None:
+            arr = (C.c_int * 3)(*[int(x) for x in shape])
+        check(self._lib.oskar_b200_tune_launch(
+            self.handle, arr, cur), "tune_launch")
+        return tuple(cur)
 
     def stats(self) -> Stats:
         s = Stats()

@@ -185,12 +185,16 @@ typedef struct oskar_B200Options
     int accum_mode;      /* OSKAR_B200_ACCUM_* */
     int apply_weight;    /* 0: ignore weight (reference); 1: vis and norm x weight */
     int classes_per_thread; /* 0: autotuned table; 1-6 or 8 forces it */
-    int staging;         /* 0: auto; 1: TMA bulk copy to shared; 2: L1 reads */
+    int staging;         /* 0: auto (the workspace's tuned choice, else L1);
+                          * 1: TMA bulk copy to shared; 2: L1 reads */
     int compensate_radius; /* ACCUM_COMPENSATED: compensate only work whose
                             * footprint centre lies within this many cells of
                             * the grid centre (the heavily hit cells);
-                            * 0: everywhere */
-    int reserved0;
+                            * 0: everywhere; -1: the workspace's tuned
+                            * radius (everywhere until tuned) */
+    int tile_shift;      /* log2 of the coarse grid tile side in cells that
+                          * orders the work (6-15); 0: the workspace's
+                          * tuned value, else grid_size / 16 (at least 64) */
     double frequency_hz; /* > 0: uu, vv, ww are in metres; they are scaled to
                           * wavelengths by frequency_hz / c in the data's
                           * precision before placement, exactly as
@@ -398,16 +402,27 @@ typedef struct oskar_B200Stats
 OSKAR_B200_EXPORT int oskar_b200_last_stats(oskar_B200Workspace* ws,
         oskar_B200Stats* stats);
 
-/* Autotuner: for each support size of `cube`, grids the sample job's
- * visibilities on planes of that support alone with every built
- * classes-per-thread choice (1-6, 8: how many footprint rows a thread of the
- * gridding kernel owns), times the gridding kernel with CUDA events (best
- * of three) and keeps the fastest per support in the workspace.  Supports
- * with fewer than 2000 sample visibilities keep the cost-model choice.
- * Later gridding calls on this workspace with classes_per_thread = 0 use
- * the table.  Device arrays as oskar_b200_grid; `grid` is scratch (its
- * contents are destroyed).  Synchronous.  table_out (host, 128 entries,
- * indexed by support, may be NULL) receives the table. */
+/* Autotuner.  (1) Threads per grid point: for each support size of `cube`,
+ * grids the sample job's visibilities on planes of that support alone with
+ * every built classes-per-thread choice (1-6, 8: how many footprint rows a
+ * thread of the gridding kernel owns), times the gridding kernel with CUDA
+ * events (best of three) and keeps the fastest per support.  Supports with
+ * fewer than 2000 sample visibilities keep the cost-model choice.  (2) Tile
+ * width and kernel-value path: grids the whole sample with the coarse tile
+ * at the automatic width, half and twice it, each with kernel values read
+ * through L1 and staged in shared memory (plain accumulation only), and
+ * keeps the fastest pipeline.  (3) Flush policy, with ACCUM_COMPENSATED in
+ * `opt`: grids the sample with compensation everywhere, nowhere, and within
+ * the radii (cells from the grid centre) holding 50, 75 and 90 % of its
+ * visibilities, and keeps the smallest radius whose grid is within a
+ * quarter of the uncompensated grid's distance from the fully compensated
+ * one (two extra grids of scratch device memory).  Later calls on this
+ * workspace that leave these to it (classes_per_thread 0, tile_shift 0,
+ * staging 0, compensate_radius -1) use the results; oskar_b200_tune_launch
+ * reads (2) and (3).  Device arrays as oskar_b200_grid; `grid` is scratch
+ * (its contents are destroyed).  Synchronous.  table_out (host, 128
+ * entries, indexed by support, may be NULL) receives the classes-per-thread
+ * table. */
 OSKAR_B200_EXPORT int oskar_b200_autotune(oskar_B200Workspace* ws,
         const oskar_B200Cube* cube, const oskar_B200Options* opt,
         size_t num_points, const void* uu, const void* vv, const void* ww,
@@ -418,6 +433,17 @@ OSKAR_B200_EXPORT int oskar_b200_autotune(oskar_B200Workspace* ws,
  * into `current` (the cost model's until one is set or tuned). */
 OSKAR_B200_EXPORT int oskar_b200_tune_table(oskar_B200Workspace* ws,
         const unsigned char* table, unsigned char* current);
+
+/* The launch shape oskar_b200_autotune picks beside the table, used by
+ * later calls whose options leave it to the workspace (tile_shift 0,
+ * staging 0, compensate_radius -1): {tile_shift, staging, compensate_radius}
+ * with staging 1 (shared) or 2 (L1).  `set` (3 ints, NULL leaves them)
+ * installs a shape; `current` (3 ints, may be NULL) receives the shape in
+ * use, {0, 2, 0} (automatic tiles, L1, compensation everywhere) until one is
+ * tuned or set.  The reference's tiled gridder fixes its tile shape at
+ * compile time (OskarTuningParams, oskar_grid_wproj_gpu.cu.old:1646-1655). */
+OSKAR_B200_EXPORT int oskar_b200_tune_launch(oskar_B200Workspace* ws,
+        const int* set, int* current);
 
 /* Statistics level of every later gridding call on this workspace:
  * 0 = none; bit 0 (1) = CUDA events between the stages (stage times in
