@@ -873,8 +873,8 @@ def run_serving(args, world, rank, local):
             "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None,
             "dtype": "f16 kernels, f32" if f16 else "f32", "data": DATA_DESC,
-            "config": {"workload": SERVING_DESC.format(
-                           kt="FP16" if f16 else "FP32"), "jobs": num_jobs,
+            "config": {"workload": SERVING_DESC.replace(
+                           "{kt}", "FP16" if f16 else "FP32"), "jobs": num_jobs,
                        "points": points, "slots": args.serving_slots,
                        "max_batch": args.serving_batch},
             "capacity_jobs_per_s": capacity,

@@ -215,7 +215,9 @@ def place(w: dict, single: bool = False):
     with FP64 coordinates, or the reference _f's float ones if single."""
     lib = oracle_lib()
     dt = np.float32 if single else np.float64
-    a = _arrays(w, dt)
+    # placement needs only the coordinates and the support table
+    a = {k: np.ascontiguousarray(w[k], dtype=dt) for k in ("uu", "vv", "ww")}
+    a["support"] = np.ascontiguousarray(w["support"], dtype=np.int32)
     n = a["uu"].shape[0]
     outs = [np.zeros(n, np.int32) for _ in range(6)] + \
         [np.zeros(n, np.int8), np.zeros(n, np.uint8)]
