@@ -21,6 +21,7 @@
 // (oskar_grid_wproj.c:104-123), summed in a different order.
 #include <algorithm>
 #include <mutex>
+#include <type_traits>
 
 #include "common.cuh"
 #include "grid_romein.cuh"
@@ -275,6 +276,24 @@ template <typename GT>
 struct PlainFlush
 {
     GT* grid;
+    // FP32: the compare, the predicated reduction and the reset of the
+    // running sum in one block of PTX.  When `valid` and cell != cur, the
+    // sum goes to cur's grid cell and restarts from zero.
+    __device__ __forceinline__ void flush_reset(int valid, unsigned cell,
+                                                unsigned cur, float& ax,
+                                                float& ay) const
+    {
+        asm volatile("{\n\t.reg .pred v, p;\n\t"
+                     "setp.ne.s32 v, %5, 0;\n\t"
+                     "setp.ne.and.u32 p, %2, %3, v;\n\t"
+                     "@p red.relaxed.gpu.global.add.v2.f32 [%4], {%0, %1};\n\t"
+                     "@p mov.f32 %0, 0f00000000;\n\t"
+                     "@p mov.f32 %1, 0f00000000;\n\t}"
+                     : "+f"(ax), "+f"(ay)
+                     : "r"(cell), "r"(cur),
+                       "l"(reinterpret_cast<float*>(grid) + 2 * (size_t)cur),
+                       "r"(valid));
+    }
     __device__ __forceinline__ void operator()(bool pred, unsigned cell, GT re,
                                                GT im) const
     {
@@ -342,8 +361,18 @@ __device__ __forceinline__ void process_task(const TapVis<GT>* __restrict__ s_vi
         typename Vec2<GT>::type acc[CPT];   // (re, im) of each row's cell
         unsigned cur[CPT];
         // Rows of this thread in this pass: b0 + q * groups, q < rows_here.
+        // Every row slot runs the same straight-line code (a per-slot
+        // `break` cost a branch and convergence barriers per tap: 19.9 ->
+        // 16.8 ms at plain_large without it); slots past the thread's rows
+        // read a clamped, in-bounds row and never flush.
         int rows_here = (w - b0 + lay.groups - 1) / lay.groups;
         rows_here = rows_here < 0 ? 0 : (rows_here > CPT ? CPT : rows_here);
+        int bq[CPT];
+#pragma unroll
+        for (int q = 0; q < CPT; ++q)
+            bq[q] = min(b0 + q * lay.groups, w - 1);
+        constexpr bool kFused =
+            std::is_same<FL, PlainFlush<float>>::value && !COUNT;
         {
             // The first visibility's cells: its taps flush nothing.
             const TapVis<GT> v = s_vis[i0];
@@ -352,9 +381,8 @@ __device__ __forceinline__ void process_task(const TapVis<GT>* __restrict__ s_vi
 #pragma unroll
             for (int q = 0; q < CPT; ++q)
             {
-                const int b = b0 + q * lay.groups;
-                const unsigned rv = min((unsigned)(b + v.mv),
-                                        (unsigned)(b + v.mv - w));
+                const unsigned rv = min((unsigned)(bq[q] + v.mv),
+                                        (unsigned)(bq[q] + v.mv - w));
                 cur[q] = v.origin + ru + rv * (unsigned)grid_size;
                 acc[q].x = acc[q].y = GT(0);
             }
@@ -369,42 +397,43 @@ __device__ __forceinline__ void process_task(const TapVis<GT>* __restrict__ s_vi
             const int kbase = v.rowbase - row_shift + col;
             const unsigned cell0 = v.origin + ru;
             // All of this visibility's kernel values for the thread's rows
-            // are requested before any is used (predicated, not branched).
+            // are requested before any is used.
             unsigned rvs[CPT];
             typename KernelLoad<KT>::Wide kv[CPT];
 #pragma unroll
             for (int q = 0; q < CPT; ++q)
             {
-                const int b = b0 + q * lay.groups;
-                rvs[q] = min((unsigned)(b + v.mv), (unsigned)(b + v.mv - w));
-                KT raw{};
-                if (q < rows_here) raw = slab[kbase + (int)rvs[q] * pitch];
-                kv[q] = KernelLoad<KT>::get(raw);
+                rvs[q] = min((unsigned)(bq[q] + v.mv),
+                             (unsigned)(bq[q] + v.mv - w));
+                kv[q] = KernelLoad<KT>::get(slab[kbase + (int)rvs[q] * pitch]);
             }
 #pragma unroll
             for (int q = 0; q < CPT; ++q)
             {
-                if (q >= rows_here) break;
-                const auto k = kv[q];
                 const unsigned cell = cell0 + rvs[q] * (unsigned)grid_size;
-                const bool change = cell != cur[q];
-                flush(change, cur[q], acc[q].x, acc[q].y);
-                if (COUNT) flushes += change;
-                acc[q].x = change ? GT(0) : acc[q].x;
-                acc[q].y = change ? GT(0) : acc[q].y;
+                if constexpr (kFused)
+                {
+                    flush.flush_reset(q < rows_here, cell, cur[q], acc[q].x,
+                                      acc[q].y);
+                }
+                else
+                {
+                    const bool change = q < rows_here && cell != cur[q];
+                    flush(change, cur[q], acc[q].x, acc[q].y);
+                    if (COUNT) flushes += change;
+                    acc[q].x = change ? GT(0) : acc[q].x;
+                    acc[q].y = change ? GT(0) : acc[q].y;
+                }
                 cur[q] = cell;
                 typename Vec2<GT>::type kk;
-                kk.x = (GT)k.x;
-                kk.y = (GT)k.y;
+                kk.x = (GT)kv[q].x;
+                kk.y = (GT)kv[q].y;
                 cmac(acc[q], v.c0, v.c1, kk);
             }
         }
 #pragma unroll
         for (int q = 0; q < CPT; ++q)
-        {
-            if (q >= rows_here) break;
-            flush(true, cur[q], acc[q].x, acc[q].y);
-        }
+            flush(q < rows_here, cur[q], acc[q].x, acc[q].y);
         if (COUNT) flushes += rows_here > 0 ? rows_here : 0;
     }
 }
@@ -685,6 +714,21 @@ cudaError_t launch_variant(const GridArgs& a, int num_sms, size_t smem,
             e = cudaFuncSetAttribute(
                 fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return e;
+            if (!STAGED)
+            {
+                // Only the shared memory 3 CTAs need; the rest of the SM's
+                // unified L1/shared storage caches kernel values (measured
+                // 19.88 -> 19.66 ms at plain_large against the default).
+                cudaFuncAttributes fa{};
+                e = cudaFuncGetAttributes(&fa, fn);
+                if (e != cudaSuccess) return e;
+                const size_t per = smem + fa.sharedSizeBytes + 1024;
+                int pct = (int)((100 * 3 * per + 228 * 1024 - 1) / (228 * 1024));
+                pct = pct > 100 ? 100 : pct;
+                e = cudaFuncSetAttribute(
+                    fn, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+                if (e != cudaSuccess) return e;
+            }
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
                 &per_sm, fn, kGridThreads, smem);
             if (e != cudaSuccess) return e;
