@@ -104,22 +104,6 @@ __device__ __forceinline__ PlaceConsts place_consts(const JobDesc& jd)
     return pc;
 }
 
-// 16 bytes of consecutive values from a 16-byte aligned address.
-__device__ __forceinline__ void load16(const float* p, float (&v)[4])
-{
-    const float4 x = __ldg(reinterpret_cast<const float4*>(p));
-    v[0] = x.x;
-    v[1] = x.y;
-    v[2] = x.z;
-    v[3] = x.w;
-}
-__device__ __forceinline__ void load16(const double* p, double (&v)[2])
-{
-    const double2 x = __ldg(reinterpret_cast<const double2*>(p));
-    v[0] = x.x;
-    v[1] = x.y;
-}
-
 template <typename T, int MODE>
 __global__ void __launch_bounds__(kPrepThreads)
 prep_kernel(const PrepArgs a)
@@ -148,79 +132,47 @@ prep_kernel(const PrepArgs a)
     unsigned long long* job_hist = a.plane_counts + (size_t)job * a.max_planes;
     double norm = 0.0;
     unsigned skipped = 0;
-    // Each thread takes kVec consecutive points, reading their coordinates
-    // with one 16-byte load per array when the three arrays are 16-byte
-    // aligned (scalar loads otherwise, and for a ragged end).  The block's
-    // loop bounds are the same for all its threads, so every lane takes part
-    // in the warp-wide histogram step below.
-    constexpr int kVec = 16 / (int)sizeof(T);
-    const bool vec_ok = ((reinterpret_cast<uintptr_t>(uu) |
-                          reinterpret_cast<uintptr_t>(vv) |
-                          reinterpret_cast<uintptr_t>(ww)) & 15u) == 0;
-    const size_t chunk = (size_t)blockDim.x * kVec;
-    for (size_t base = (size_t)blockIdx.x * chunk; base < n;
-         base += (size_t)gridDim.x * chunk)
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t base = (size_t)blockIdx.x * blockDim.x; base < n;
+         base += stride)
     {
-        const size_t i0 = base + (size_t)threadIdx.x * kVec;
-        T cu[kVec], cv[kVec], cw[kVec];
-        if (vec_ok && i0 + kVec <= n)
+        const size_t i = base + threadIdx.x;
+        const bool in_range = i < n;
+        const size_t g = first + i;
+        Placed p{};
+        if (in_range)
+            p = place_one<T, MODE>(scale_coord(uu[i], jd),
+                                   scale_coord(vv[i], jd),
+                                   scale_coord(ww[i], jd), pc, jd.support);
+        const bool keep = in_range && !p.skipped;
+        if (in_range)
         {
-            load16(uu + i0, cu);
-            load16(vv + i0, cv);
-            load16(ww + i0, cw);
+            if (keep)
+            {
+                a.rec[g] = make_int4(p.gu, p.gv,
+                                     p.plane | (p.conj < 0 ? (int)0x80000000 : 0),
+                                     (p.off_u + half) | ((p.off_v + half) << 16));
+                a.keys[g] = make_key(a.key, job, p.gu, p.gv, p.plane);
+                double s = jd.norm_table[((size_t)p.plane * span +
+                                          (p.off_v + half)) * span +
+                                         (p.off_u + half)];
+                if (a.apply_weight) s *= (double)wt[i];
+                norm += s;
+            }
+            else
+            {
+                a.keys[g] = skip_key;
+            }
+            a.vals[g] = (uint32_t)g;
         }
-        else
+        skipped += in_range && !keep;
+        // plane histogram, aggregated across equal planes in the warp
+        const unsigned pl = keep ? (unsigned)p.plane : 0xffffffffu;
+        const unsigned peers = __match_any_sync(0xffffffffu, pl);
+        if (keep && lane == __ffs(peers) - 1)
         {
-#pragma unroll
-            for (int j = 0; j < kVec; ++j)
-            {
-                const bool ok = i0 + j < n;
-                cu[j] = ok ? uu[i0 + j] : T(0);
-                cv[j] = ok ? vv[i0 + j] : T(0);
-                cw[j] = ok ? ww[i0 + j] : T(0);
-            }
-        }
-#pragma unroll
-        for (int j = 0; j < kVec; ++j)
-        {
-            const size_t i = i0 + j;
-            const bool in_range = i < n;
-            const size_t g = first + i;
-            Placed p{};
-            if (in_range)
-                p = place_one<T, MODE>(scale_coord(cu[j], jd),
-                                       scale_coord(cv[j], jd),
-                                       scale_coord(cw[j], jd), pc, jd.support);
-            const bool keep = in_range && !p.skipped;
-            if (in_range)
-            {
-                if (keep)
-                {
-                    a.rec[g] = make_int4(p.gu, p.gv,
-                                         p.plane | (p.conj < 0 ? (int)0x80000000 : 0),
-                                         (p.off_u + half) | ((p.off_v + half) << 16));
-                    a.keys[g] = make_key(a.key, job, p.gu, p.gv, p.plane);
-                    double s = jd.norm_table[((size_t)p.plane * span +
-                                              (p.off_v + half)) * span +
-                                             (p.off_u + half)];
-                    if (a.apply_weight) s *= (double)wt[i];
-                    norm += s;
-                }
-                else
-                {
-                    a.keys[g] = skip_key;
-                }
-                a.vals[g] = (uint32_t)g;
-            }
-            skipped += in_range && !keep;
-            // plane histogram, aggregated across equal planes in the warp
-            const unsigned pl = keep ? (unsigned)p.plane : 0xffffffffu;
-            const unsigned peers = __match_any_sync(0xffffffffu, pl);
-            if (keep && lane == __ffs(peers) - 1)
-            {
-                if (smem_hist) atomicAdd(&s_hist[pl], (unsigned)__popc(peers));
-                else atomicAdd(&job_hist[pl], (unsigned long long)__popc(peers));
-            }
+            if (smem_hist) atomicAdd(&s_hist[pl], (unsigned)__popc(peers));
+            else atomicAdd(&job_hist[pl], (unsigned long long)__popc(peers));
         }
     }
     norm = warp_sum(norm);
