@@ -892,7 +892,7 @@ int oskar_b200_tune_table(oskar_B200Workspace* ws, const unsigned char* table,
     if (table)
     {
         for (int s = 0; s < 128; ++s)
-            if (!((table[s] >= 1 && table[s] <= 6) || table[s] == 8))
+            if (!(table[s] >= 1 && table[s] <= 6))
                 return OSKAR_B200_ERR_INVALID_ARGUMENT;
         memcpy(ws->tune, table, sizeof(ws->tune));
         ws->tuned = 1;

@@ -33,7 +33,7 @@ namespace b200 {
 
 namespace {
 
-constexpr int kChoices[] = {1, 2, 3, 4, 5, 6, 8};
+constexpr int kChoices[] = {1, 2, 3, 4, 5, 6};
 constexpr size_t kMinPoints = 2000;   // fewer: keep the model's choice
 constexpr int kRepeats = 3;           // best of three launches
 

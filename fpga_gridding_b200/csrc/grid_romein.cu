@@ -455,7 +455,6 @@ __device__ __forceinline__ void dispatch_cpt(int cpt, const TapVis<GT>* s_vis,
     case 3: B200_CPT(3); break;
     case 4: B200_CPT(4); break;
     case 6: B200_CPT(6); break;
-    case 8: B200_CPT(8); break;
     default: B200_CPT(5); break;
     }
 #undef B200_CPT
@@ -485,10 +484,12 @@ __device__ __forceinline__ CompensatedFlush make_flush<float, true>(void* grid, 
                             active};
 }
 
-// At least 3 CTAs per SM (<= 85 registers): measured faster on plain_large
-// than 4 CTAs with spills or 2 CTAs unconstrained.
+// At least grid_ctas_per_sm<GT>() CTAs per SM.  FP32: with the
+// straight-line row slots and at most 6 rows per thread, 4 CTAs (64
+// registers) measured 16.28 ms at plain_large against 16.76 ms for 3 (and
+// 16.94-17.74 ms for 5 or 6 CTAs with at most 4 or 3 rows per thread).
 template <typename GT, typename KT, bool STAGED, bool COMP, bool COUNT>
-__global__ void __launch_bounds__(kGridThreads, 3)
+__global__ void __launch_bounds__(kGridThreads, grid_ctas_per_sm<GT>())
 romein_grid_kernel(const GridArgs a)
 {
     using V2 = typename Vec2<GT>::type;
@@ -716,14 +717,17 @@ cudaError_t launch_variant(const GridArgs& a, int num_sms, size_t smem,
             if (e != cudaSuccess) return e;
             if (!STAGED)
             {
-                // Only the shared memory 3 CTAs need; the rest of the SM's
-                // unified L1/shared storage caches kernel values (measured
-                // 19.88 -> 19.66 ms at plain_large against the default).
+                // Only the shared memory grid_ctas_per_sm CTAs need; the
+                // rest of the SM's unified L1/shared storage caches kernel
+                // values (measured 19.88 -> 19.66 ms at plain_large against
+                // the default carveout).
                 cudaFuncAttributes fa{};
                 e = cudaFuncGetAttributes(&fa, fn);
                 if (e != cudaSuccess) return e;
                 const size_t per = smem + fa.sharedSizeBytes + 1024;
-                int pct = (int)((100 * 3 * per + 228 * 1024 - 1) / (228 * 1024));
+                int pct = (int)((100 * grid_ctas_per_sm<GT>() * per +
+                                 228 * 1024 - 1) /
+                                (228 * 1024));
                 pct = pct > 100 ? 100 : pct;
                 e = cudaFuncSetAttribute(
                     fn, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
@@ -753,7 +757,7 @@ cudaError_t launch_variant(const GridArgs& a, int num_sms, size_t smem,
 // CTA's thread slots holding a live class.
 void default_tune_table(unsigned char* cpt)
 {
-    const int choices[] = {1, 2, 3, 4, 5, 6, 8};
+    const int choices[] = {1, 2, 3, 4, 5, 6};
     for (int s = 0; s < kTuneMax; ++s)
     {
         const int w = 2 * s + 1;

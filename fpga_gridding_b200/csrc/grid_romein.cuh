@@ -6,6 +6,11 @@
 namespace b200 {
 
 constexpr int kGridThreads = 256;   // threads per CTA
+// Resident CTAs per SM the gridding kernel's registers are bounded for:
+// 4 for FP32 grids (64 registers), 3 for FP64 (80; its accumulators and
+// coefficients are twice as wide and spill at 64).
+template <typename GT>
+constexpr int grid_ctas_per_sm() { return sizeof(GT) == 8 ? 3 : 4; }
 constexpr int kTaskMax = 256;       // visibilities per task
 constexpr int kTuneMax = 128;       // supports covered by the tune table
 constexpr unsigned kBulkChunk = 32768;  // bytes per cp.async.bulk

@@ -366,8 +366,7 @@ int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
     // Counting the grid atomics costs an instruction per tap: only when the
     // caller asked for it (statistics level bit 1).
     ga.count_flushes = (ws->stage_timing & 2) ? 1 : 0;
-    if ((opt->classes_per_thread >= 1 && opt->classes_per_thread <= 6) ||
-        opt->classes_per_thread == 8)
+    if (opt->classes_per_thread >= 1 && opt->classes_per_thread <= 6)
         memset(ga.cpt, opt->classes_per_thread, sizeof(ga.cpt));
     else if (ws->tuned)
         memcpy(ga.cpt, ws->tune, sizeof(ga.cpt));

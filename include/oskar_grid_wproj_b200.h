@@ -184,7 +184,7 @@ typedef struct oskar_B200Options
     int kernel_type;     /* OSKAR_B200_KERNEL_* */
     int accum_mode;      /* OSKAR_B200_ACCUM_* */
     int apply_weight;    /* 0: ignore weight (reference); 1: vis and norm x weight */
-    int classes_per_thread; /* 0: autotuned table; 1-6 or 8 forces it */
+    int classes_per_thread; /* 0: autotuned table; 1-6 forces it */
     int staging;         /* 0: auto (the workspace's tuned choice, else L1);
                           * 1: TMA bulk copy to shared; 2: L1 reads */
     int compensate_radius; /* ACCUM_COMPENSATED: compensate only work whose
@@ -404,7 +404,7 @@ OSKAR_B200_EXPORT int oskar_b200_last_stats(oskar_B200Workspace* ws,
 
 /* Autotuner.  (1) Threads per grid point: for each support size of `cube`,
  * grids the sample job's visibilities on planes of that support alone with
- * every built classes-per-thread choice (1-6, 8: how many footprint rows a
+ * every built classes-per-thread choice (1-6: how many footprint rows a
  * thread of the gridding kernel owns), times the gridding kernel with CUDA
  * events (best of three) and keeps the fastest per support.  Supports with
  * fewer than 2000 sample visibilities keep the cost-model choice.  (2) Tile
@@ -429,7 +429,7 @@ OSKAR_B200_EXPORT int oskar_b200_autotune(oskar_B200Workspace* ws,
         const void* vis, double cell_size_rad, double w_scale, int grid_size,
         void* grid, unsigned char* table_out);
 /* Sets the workspace's classes-per-thread table (128 entries indexed by
- * support, each 1-6 or 8; NULL leaves it) and/or copies the table in use
+ * support, each 1-6; NULL leaves it) and/or copies the table in use
  * into `current` (the cost model's until one is set or tuned). */
 OSKAR_B200_EXPORT int oskar_b200_tune_table(oskar_B200Workspace* ws,
         const unsigned char* table, unsigned char* current);

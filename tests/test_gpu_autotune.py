@@ -14,7 +14,7 @@ from fpga_gridding_b200 import workloads as W
 
 pytestmark = pytest.mark.gpu
 
-ALLOWED = {1, 2, 3, 4, 5, 6, 8}
+ALLOWED = {1, 2, 3, 4, 5, 6}
 
 
 def test_autotune_then_grid_matches_oracle(oracle):
