@@ -726,7 +726,8 @@ def run_serving(args, world, rank, local):
     from fpga_gridding_b200.serving import Server
 
     num_jobs = args.serving_jobs
-    base, jobs, specs = W.serving_stream(num_jobs=num_jobs, seed=4 + rank,
+    base, jobs, specs = W.serving_stream(num_jobs=num_jobs,
+                                         seed=4 + rank + args.serving_seed,
                                          device="cuda")
     ws = fg.Workspace(local)
     cubes = {}
@@ -749,7 +750,7 @@ def run_serving(args, world, rank, local):
                    base["weight"][s:e], j["cell_size_rad"], j["w_scale"],
                    j["grid_size"])
 
-    rng = np.random.default_rng(123 + rank)
+    rng = np.random.default_rng(123 + rank + args.serving_seed)
     audited = set(rng.choice(num_jobs, size=max(1, num_jobs // 20),
                              replace=False).tolist())
     alone_grids = {}
@@ -875,6 +876,7 @@ def run_serving(args, world, rank, local):
             "dtype": "f16 kernels, f32" if f16 else "f32", "data": DATA_DESC,
             "config": {"workload": SERVING_DESC.replace(
                            "{kt}", "FP16" if f16 else "FP32"), "jobs": num_jobs,
+                       "seed": args.serving_seed,
                        "points": points, "slots": args.serving_slots,
                        "max_batch": args.serving_batch},
             "capacity_jobs_per_s": capacity,
@@ -1468,6 +1470,9 @@ def main():
                     help="concurrent batches the server keeps on the GPU")
     ap.add_argument("--serving-batch", type=int, default=32,
                     help="most jobs the server puts in one batch")
+    ap.add_argument("--serving-seed", type=int, default=0,
+                    help="offset of the serving stream's seeds (job mix, "
+                         "arrivals, audited jobs)")
     ap.add_argument("--serving-kernel", choices=("f32", "f16"),
                     default="f32",
                     help="kernel-cube storage of the serving jobs (FP16 "
