@@ -130,25 +130,36 @@ degrid_kernel(const uint32_t* __restrict__ order,
                     static_cast<const C2*>(jd->grid) + (size_t)v0 * G + u0;
                 // The group's lanes walk the W * W taps in row-major order,
                 // kGroup at a time (contiguous grid reads within a row).
+                // The lane's tap (j, k) is tracked as 32-bit running
+                // offsets (grid cell j * G + k, kernel row j * pitch),
+                // stepped kGroup taps at a time with k wrapping past W: the
+                // 64-bit index arithmetic per tap cost 28.4 -> 26.5 ms at
+                // plain_large.
                 const int taps = W * W, dj = kGroup / W, dk = kGroup % W;
-                int j = gl / W, k = gl - (gl / W) * W;
+                const int j0 = gl / W;
+                int k = gl - j0 * W;
+                unsigned goff = (unsigned)j0 * (unsigned)G + (unsigned)k;
+                unsigned krow = (unsigned)j0 * (unsigned)d.pitch;
+                const unsigned gstep = (unsigned)dj * (unsigned)G + (unsigned)dk;
+                const unsigned kstep = (unsigned)dj * (unsigned)d.pitch;
+                const unsigned gwrap = (unsigned)G - (unsigned)W;
+                const unsigned kwrap = (unsigned)d.pitch;
 #pragma unroll 4
                 for (int t = gl; t < taps; t += kGroup)
                 {
-                    const auto kv = KernelLoad<KT>::get(
-                        slab[j * d.pitch + pos[k]]);
-                    const C2 g = grid[(size_t)j * G + k];
+                    const auto kv = KernelLoad<KT>::get(slab[krow + pos[k]]);
+                    const C2 g = grid[goff];
                     const GT kr = (GT)kv.x, ki = sgn * (GT)kv.y;
                     // grid * conj(Kt), Kt = (kr, ki)
                     are = fma(g.x, kr, fma(g.y, ki, are));
                     aim = fma(g.y, kr, fma(-g.x, ki, aim));
                     k += dk;
-                    j += dj;
-                    if (k >= W)
-                    {
-                        k -= W;
-                        ++j;
-                    }
+                    goff += gstep;
+                    krow += kstep;
+                    const bool wrap = k >= W;
+                    k = wrap ? k - W : k;
+                    goff += wrap ? gwrap : 0u;
+                    krow += wrap ? kwrap : 0u;
                 }
             }
 #pragma unroll
