@@ -95,16 +95,40 @@ def measured_peaks():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per launch of the gridding kernel from the committed ncu
+def profiled_value(key):
+    """A per-launch figure of the gridding kernel from the committed ncu
     summary (profiles/romein_grid_kernel_plain_large.md), or None."""
     p = os.path.join(ROOT, "profiles", "romein_grid_kernel_plain_large.md")
     try:
         text = open(p).read()
     except OSError:
         return None
-    m = re.search(r"dram_bytes_per_launch_full_job:\s*([0-9.eE+]+)", text)
+    m = re.search(key + r":\s*([0-9.eE+]+)", text)
     return float(m.group(1)) if m else None
+
+
+def profiled_traffic():
+    """DRAM bytes (read + write) of one full-size gridding launch."""
+    return profiled_value("dram_bytes_per_launch_full_job")
+
+
+def issue_peak_per_s(device=0):
+    """Warp instructions the device can issue per second: 4 schedulers per
+    SM, one instruction each per cycle, at the maximum SM clock."""
+    props = torch.cuda.get_device_properties(device)
+    mhz = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            mhz = float(json.load(f)["sm_max_mhz"])
+    except Exception:
+        out = subprocess.run(["nvidia-smi", "--query-gpu=clocks.max.sm",
+                              "--format=csv,noheader,nounits", "-i",
+                              str(device)], capture_output=True, text=True)
+        try:
+            mhz = float(out.stdout.strip().splitlines()[0])
+        except (ValueError, IndexError):
+            return None
+    return props.multi_processor_count * 4 * mhz * 1e6
 
 
 class ClockSampler:
@@ -360,6 +384,20 @@ def run_b200(args, world, rank, local):
                                   "measured in this run)",
                 "algorithmic_bytes_per_launch": alg_bytes,
                 "kernel_ms": round(kernel_ms, 3)}
+    # The ceiling that binds: instruction issue.  Warp instructions of one
+    # full-size launch (ncu smsp__inst_executed.sum, copied from the
+    # profile) over this run's kernel time, against the issue rate.
+    winst = profiled_value("warp_instructions_per_launch_full_job")
+    ipeak = issue_peak_per_s(local)
+    if winst and ipeak:
+        roofline["issue"] = {
+            "achieved_warp_inst_per_s": winst / (kernel_ms * 1e-3),
+            "peak_warp_inst_per_s": ipeak,
+            "frac": round(winst / (kernel_ms * 1e-3) / ipeak, 4),
+            "warp_instructions_per_launch": winst,
+            "source": "ncu smsp__inst_executed.sum of one full-size launch, "
+                      "copied from profiles/romein_grid_kernel_plain_large.md"
+                      "; peak = SMs x 4 schedulers x max SM clock"}
     # L2-atomic roofline: measured complex-FP32 red.v2 rate on an
     # L2-resident 2048^2 grid.
     rate = C.c_double(0.0)
