@@ -34,42 +34,82 @@ constexpr int kGroups = 32 / kGroup;
 constexpr int kDegridMaxW = 255;   // footprint width for support <= 127
 constexpr int kDegridChunk = 128;  // visibilities per work-queue item
 
+// Sum over taps of grid * conj(Kt), Kt = (kr, sgn * ki).  FP32: two packed
+// FMAs per tap, A += g * kr and B += g * ki, with the sign applied once at
+// the end (re = A.x + sgn B.y, im = A.y - sgn B.x).  FP64: four FMAs per
+// tap in the order of the definition.
+template <typename GT> struct DegridAcc;
+template <> struct DegridAcc<float>
+{
+    float2 a = make_float2(0.f, 0.f), b = make_float2(0.f, 0.f);
+    float sgn;
+    __device__ __forceinline__ explicit DegridAcc(float s) : sgn(s) {}
+    __device__ __forceinline__ void add(const float2 g, float kr, float ki)
+    {
+        a = __ffma2_rn(g, make_float2(kr, kr), a);
+        b = __ffma2_rn(g, make_float2(ki, ki), b);
+    }
+    __device__ __forceinline__ void finish(float& re, float& im) const
+    {
+        re = fmaf(sgn, b.y, a.x);
+        im = fmaf(-sgn, b.x, a.y);
+    }
+};
+template <> struct DegridAcc<double>
+{
+    double re = 0.0, im = 0.0, sgn;
+    __device__ __forceinline__ explicit DegridAcc(double s) : sgn(s) {}
+    __device__ __forceinline__ void add(const double2 g, double kr, double ki)
+    {
+        ki *= sgn;
+        re = fma(g.x, kr, fma(g.y, ki, re));
+        im = fma(g.y, kr, fma(-g.x, ki, im));
+    }
+    __device__ __forceinline__ void finish(double& r, double& i) const
+    {
+        r = re;
+        i = im;
+    }
+};
+
 // Rows in the outer loop, each lane of a group owning the footprint columns
-// k = gl + kGroup * m, m < M: the kernel column position and the grid column
-// of each are registers, so a tap costs two addresses, two loads and the
-// multiply-adds.  Used for footprints kGroup to 5 * kGroup wide (narrower
-// ones would leave lanes idle; wider ones take the flattened walk).
+// k = gl + kGroup * m, m < M: the byte addresses of each column's kernel
+// value and grid cell in the first row are registers, so a tap costs two
+// wide multiply-adds (row times the row pitch in bytes), two loads and the
+// packed multiply-adds.  Used for footprints kGroup to 5 * kGroup wide
+// (narrower ones would leave lanes idle; wider ones take the flattened
+// walk).  The slab and the grid are read-only here: non-coherent loads.
 template <int M, typename GT, typename KT, typename C2>
 __device__ __forceinline__ void degrid_rows(const KT* __restrict__ slab,
                                             const C2* __restrict__ grid,
                                             int W, int pitch, int G,
-                                            const short* pos, int gl, GT sgn,
-                                            GT& are, GT& aim)
+                                            const short* pos, int gl,
+                                            DegridAcc<GT>& acc)
 {
-    unsigned kc[M], gc[M];
+    const char* kc[M];
+    const char* gc[M];
     bool ok[M];
 #pragma unroll
     for (int m = 0; m < M; ++m)
     {
         const int k = gl + kGroup * m;
         ok[m] = k < W;
-        kc[m] = ok[m] ? (unsigned)pos[k] : 0u;
-        gc[m] = ok[m] ? (unsigned)k : 0u;
+        kc[m] = reinterpret_cast<const char*>(slab + (ok[m] ? pos[k] : 0));
+        gc[m] = reinterpret_cast<const char*>(grid + (ok[m] ? k : 0));
     }
+    const unsigned kb = (unsigned)pitch * (unsigned)sizeof(KT);
+    const unsigned gb = (unsigned)G * (unsigned)sizeof(C2);
     for (int j = 0; j < W; ++j)
     {
-        const KT* __restrict__ kr = slab + (size_t)j * pitch;
-        const C2* __restrict__ gr = grid + (size_t)j * G;
 #pragma unroll
         for (int m = 0; m < M; ++m)
         {
             if (!ok[m]) continue;
-            const auto kv = KernelLoad<KT>::get(kr[kc[m]]);
-            const C2 g = gr[gc[m]];
-            const GT k_r = (GT)kv.x, k_i = sgn * (GT)kv.y;
-            // grid * conj(Kt), Kt = (k_r, k_i)
-            are = fma(g.x, k_r, fma(g.y, k_i, are));
-            aim = fma(g.y, k_r, fma(-g.x, k_i, aim));
+            const auto kv = KernelLoad<KT>::get(__ldg(
+                reinterpret_cast<const KT*>(kc[m] + (size_t)j * kb)));
+            const C2 g = __ldg(
+                reinterpret_cast<const C2*>(gc[m] + (size_t)j * gb));
+            acc.add(g, (GT)kv.x, (GT)kv.y);
         }
     }
 }
@@ -160,7 +200,7 @@ degrid_kernel(const uint32_t* __restrict__ order,
                 pos[k] = (short)((x % os) * d.L + x / os);
             }
             __syncwarp();
-            GT are = GT(0), aim = GT(0);
+            DegridAcc<GT> acc(sgn);
             if (active)
             {
                 const KT* __restrict__ slab =
@@ -177,11 +217,11 @@ degrid_kernel(const uint32_t* __restrict__ order,
                     // 26.5 -> 25.2 ms)
                     switch (mc)
                     {
-                    case 1: degrid_rows<1, GT>(slab, grid, W, d.pitch, G, pos, gl, sgn, are, aim); break;
-                    case 2: degrid_rows<2, GT>(slab, grid, W, d.pitch, G, pos, gl, sgn, are, aim); break;
-                    case 3: degrid_rows<3, GT>(slab, grid, W, d.pitch, G, pos, gl, sgn, are, aim); break;
-                    case 4: degrid_rows<4, GT>(slab, grid, W, d.pitch, G, pos, gl, sgn, are, aim); break;
-                    default: degrid_rows<5, GT>(slab, grid, W, d.pitch, G, pos, gl, sgn, are, aim); break;
+                    case 1: degrid_rows<1, GT>(slab, grid, W, d.pitch, G, pos, gl, acc); break;
+                    case 2: degrid_rows<2, GT>(slab, grid, W, d.pitch, G, pos, gl, acc); break;
+                    case 3: degrid_rows<3, GT>(slab, grid, W, d.pitch, G, pos, gl, acc); break;
+                    case 4: degrid_rows<4, GT>(slab, grid, W, d.pitch, G, pos, gl, acc); break;
+                    default: degrid_rows<5, GT>(slab, grid, W, d.pitch, G, pos, gl, acc); break;
                     }
                 }
                 else
@@ -203,12 +243,10 @@ degrid_kernel(const uint32_t* __restrict__ order,
 #pragma unroll 4
                     for (int t = gl; t < taps; t += kGroup)
                     {
-                        const auto kv = KernelLoad<KT>::get(slab[krow + pos[k]]);
-                        const C2 g = grid[goff];
-                        const GT kr = (GT)kv.x, ki = sgn * (GT)kv.y;
-                        // grid * conj(Kt), Kt = (kr, ki)
-                        are = fma(g.x, kr, fma(g.y, ki, are));
-                        aim = fma(g.y, kr, fma(-g.x, ki, aim));
+                        const auto kv =
+                            KernelLoad<KT>::get(__ldg(slab + krow + pos[k]));
+                        const C2 g = __ldg(grid + goff);
+                        acc.add(g, (GT)kv.x, (GT)kv.y);
                         k += dk;
                         goff += gstep;
                         krow += kstep;
@@ -219,6 +257,8 @@ degrid_kernel(const uint32_t* __restrict__ order,
                     }
                 }
             }
+            GT are, aim;
+            acc.finish(are, aim);
 #pragma unroll
             for (int o = kGroup / 2; o > 0; o >>= 1)
             {
