@@ -72,6 +72,30 @@ template <> struct DegridAcc<double>
     }
 };
 
+// Slab column of footprint column k: the quadrant column |off_u + (k - S) os|
+// in the phase-major layout, (x mod os) * L + x / os.  For k >= tu the
+// argument is non-negative and the column is cp + k; below, cn - k.  With
+// |off_u| <= os the remainders and quotients need no division.
+struct ColumnMap
+{
+    int tu, cp, cn;
+    __device__ __forceinline__ ColumnMap(int off_u, int S, int os, int L)
+    {
+        const int rp = off_u < 0 ? off_u + os : (off_u >= os ? off_u - os : off_u);
+        const int qp = off_u < 0 ? -1 : (off_u >= os ? 1 : 0);
+        const int on = -off_u;
+        const int rn = on < 0 ? on + os : (on >= os ? on - os : on);
+        const int qn = on < 0 ? -1 : (on >= os ? 1 : 0);
+        tu = S + (off_u < 0 ? 1 : 0);
+        cp = rp * L + qp - S;
+        cn = rn * L + qn + S;
+    }
+    __device__ __forceinline__ int operator()(int k) const
+    {
+        return k >= tu ? cp + k : cn - k;
+    }
+};
+
 // Rows in the outer loop, each lane of a group owning the footprint columns
 // k = gl + kGroup * m, m < M: the byte addresses of each column's kernel
 // value and grid cell in the first row are registers, so a tap costs two
@@ -83,7 +107,7 @@ template <int M, typename GT, typename KT, typename C2>
 __device__ __forceinline__ void degrid_rows(const KT* __restrict__ slab,
                                             const C2* __restrict__ grid,
                                             int W, int pitch, int G,
-                                            const short* pos, int gl,
+                                            const ColumnMap& cm, int gl,
                                             DegridAcc<GT>& acc)
 {
     const char* kc[M];
@@ -94,7 +118,7 @@ __device__ __forceinline__ void degrid_rows(const KT* __restrict__ slab,
     {
         const int k = gl + kGroup * m;
         ok[m] = k < W;
-        kc[m] = reinterpret_cast<const char*>(slab + (ok[m] ? pos[k] : 0));
+        kc[m] = reinterpret_cast<const char*>(slab + (ok[m] ? cm(k) : 0));
         gc[m] = reinterpret_cast<const char*>(grid + (ok[m] ? k : 0));
     }
     const unsigned kb = (unsigned)pitch * (unsigned)sizeof(KT);
@@ -130,12 +154,10 @@ degrid_kernel(const uint32_t* __restrict__ order,
     using C2 = typename Cplx<GT>::type;
     // slab column position of each footprint column, per lane group (a
     // position is below the slab pitch, < 2^15 for oversample <= 32)
-    __shared__ short s_pos[kDegridWarps][kGroups][kDegridMaxW];
     __shared__ unsigned long long s_chunk;
     const size_t valid = n - counters[CNT_SKIPPED];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int group = lane / kGroup, gl = lane % kGroup;
-    short* pos = s_pos[warp][group];
     // A CTA takes chunks of kDegridChunk consecutive sorted visibilities
     // from a work queue: its warps work on neighbouring footprints and share
     // grid lines and kernel rows in L1, and the uneven cost of the chunks
@@ -195,14 +217,7 @@ degrid_kernel(const uint32_t* __restrict__ order,
                     W = 0;
                 }
             }
-            __syncwarp();   // the previous visibilities are done with pos[]
-            // quadrant column |off_u + (k - S) * os|, phase-major position
-            for (int k = gl; k < W; k += kGroup)
-            {
-                const int x = abs(off_u + (k - S) * os);
-                pos[k] = (short)((x % os) * d.L + x / os);
-            }
-            __syncwarp();
+            const ColumnMap cm(off_u, S, os, d.L);
             DegridAcc<GT> acc(sgn);
             if (active)
             {
@@ -220,11 +235,11 @@ degrid_kernel(const uint32_t* __restrict__ order,
                     // 26.5 -> 25.2 ms)
                     switch (mc)
                     {
-                    case 1: degrid_rows<1, GT>(slab, grid, W, d.pitch, G, pos, gl, acc); break;
-                    case 2: degrid_rows<2, GT>(slab, grid, W, d.pitch, G, pos, gl, acc); break;
-                    case 3: degrid_rows<3, GT>(slab, grid, W, d.pitch, G, pos, gl, acc); break;
-                    case 4: degrid_rows<4, GT>(slab, grid, W, d.pitch, G, pos, gl, acc); break;
-                    default: degrid_rows<5, GT>(slab, grid, W, d.pitch, G, pos, gl, acc); break;
+                    case 1: degrid_rows<1, GT>(slab, grid, W, d.pitch, G, cm, gl, acc); break;
+                    case 2: degrid_rows<2, GT>(slab, grid, W, d.pitch, G, cm, gl, acc); break;
+                    case 3: degrid_rows<3, GT>(slab, grid, W, d.pitch, G, cm, gl, acc); break;
+                    case 4: degrid_rows<4, GT>(slab, grid, W, d.pitch, G, cm, gl, acc); break;
+                    default: degrid_rows<5, GT>(slab, grid, W, d.pitch, G, cm, gl, acc); break;
                     }
                 }
                 else
@@ -247,7 +262,7 @@ degrid_kernel(const uint32_t* __restrict__ order,
                     for (int t = gl; t < taps; t += kGroup)
                     {
                         const auto kv =
-                            KernelLoad<KT>::get(__ldg(slab + krow + pos[k]));
+                            KernelLoad<KT>::get(__ldg(slab + krow + cm(k)));
                         const C2 g = __ldg(grid + goff);
                         acc.add(g, (GT)kv.x, (GT)kv.y);
                         k += dk;
