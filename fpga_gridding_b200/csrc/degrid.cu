@@ -152,8 +152,6 @@ degrid_kernel(const uint32_t* __restrict__ order,
               unsigned long long* __restrict__ counters, size_t n)
 {
     using C2 = typename Cplx<GT>::type;
-    // slab column position of each footprint column, per lane group (a
-    // position is below the slab pitch, < 2^15 for oversample <= 32)
     __shared__ unsigned long long s_chunk;
     const size_t valid = n - counters[CNT_SKIPPED];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;

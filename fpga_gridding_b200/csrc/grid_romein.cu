@@ -235,34 +235,39 @@ __device__ __forceinline__ void red_add_c_if(bool pred, double* addr,
 }
 
 // Thread layout of one task.  The W x W classes are split into W columns
-// (a) and W rows (b).  A thread owns one column and CPT rows, so the column
-// arithmetic of a tap is done once per visibility and shared by its CPT
-// classes, and the 32 lanes of a warp hold consecutive columns (contiguous
-// kernel reads, coalesced flushes).  `groups` threads share a column per
-// slice; thread g of a column takes rows g, g + groups, ... (CPT of them per
-// pass).  When the footprint is small, `slices` independent copies of the
-// layout split the task's visibilities between them.
+// (a) and ceil(W / CPT) row groups of CPT consecutive rows; a work item is
+// one (column, row group) pair, so the column arithmetic of a tap is done
+// once per visibility and shared by the item's CPT classes, and the 32
+// lanes of a warp hold consecutive columns (contiguous kernel reads,
+// coalesced flushes).  The last row group of a column is moved up to rows
+// W - CPT .. W - 1 and its first slots, which repeat rows of the group
+// before, are masked, so every slot reads an in-bounds kernel row.  When
+// the items fit the CTA several times, `slices` copies of the layout split
+// the task's visibilities between them; otherwise the CTA's threads take
+// the items in passes of kGridThreads.  Against one column per thread with
+// rows strided by the number of threads per column (the thread count per
+// column capped at 256 / W, so wide footprints left up to a third of the
+// CTA idle in their last pass), the plain_large gridding kernel went from
+// 15.3 to 14.4 ms: fewer idle thread slots, and no per-slot row registers.
 struct TaskLayout
 {
-    int groups, passes, slices;
+    int items, slices, per_slice;
 };
 
 template <int CPT>
 __device__ __forceinline__ TaskLayout task_layout(int w)
 {
     TaskLayout t;
-    const int need = (w + CPT - 1) / CPT;
-    if (w * need <= kGridThreads)
+    t.items = w * ((w + CPT - 1) / CPT);
+    if (t.items <= kGridThreads)
     {
-        t.groups = need;
-        t.passes = 1;
-        t.slices = kGridThreads / (w * need);
+        t.slices = kGridThreads / t.items;
+        t.per_slice = t.items;
     }
     else
     {
-        t.groups = kGridThreads / w;
-        t.passes = (w + t.groups * CPT - 1) / (t.groups * CPT);
         t.slices = 1;
+        t.per_slice = kGridThreads;
     }
     return t;
 }
@@ -358,30 +363,28 @@ __device__ __forceinline__ void process_task(const TapVis<GT>* __restrict__ s_vi
                                              int grid_size, unsigned& flushes)
 {
     const TaskLayout lay = task_layout<CPT>(w);
-    const int per_slice = w * lay.groups;
     int slices = lay.slices < m ? lay.slices : m;
-    const int r = threadIdx.x / per_slice;
+    const int r = threadIdx.x / lay.per_slice;
     if (r >= slices) return;
-    const int l = threadIdx.x - r * per_slice;
-    const int a = l % w, g = l / w;
+    const int l = threadIdx.x - r * lay.per_slice;
     const int i0 = (r * m) / slices, i1 = ((r + 1) * m) / slices;
     const unsigned pitch_b = (unsigned)pitch * (unsigned)sizeof(KT);
-    for (int pass = 0; pass < lay.passes; ++pass)
+    for (int it = l; it < lay.items; it += kGridThreads)
     {
-        const int b0 = pass * lay.groups * CPT + g;
+        const int a = it % w;
+        // Rows b0 .. b0 + CPT - 1; slots q < skip repeat the previous
+        // group's rows and never flush (CPT <= W).
+        int b0 = (it / w) * CPT, skip = 0;
+        if (b0 + CPT > w)
+        {
+            skip = b0 + CPT - w;
+            b0 = w - CPT;
+        }
+        // Every slot runs the same straight-line code (a per-slot `break`
+        // cost a branch and convergence barriers per tap: 19.9 -> 16.8 ms
+        // at plain_large without it); masked slots never flush.
         typename Vec2<GT>::type acc[CPT];   // (re, im) of each row's cell
         unsigned cur[CPT];
-        // Rows of this thread in this pass: b0 + q * groups, q < rows_here.
-        // Every row slot runs the same straight-line code (a per-slot
-        // `break` cost a branch and convergence barriers per tap: 19.9 ->
-        // 16.8 ms at plain_large without it); slots past the thread's rows
-        // read a clamped, in-bounds row and never flush.
-        int rows_here = (w - b0 + lay.groups - 1) / lay.groups;
-        rows_here = rows_here < 0 ? 0 : (rows_here > CPT ? CPT : rows_here);
-        int bq[CPT];
-#pragma unroll
-        for (int q = 0; q < CPT; ++q)
-            bq[q] = min(b0 + q * lay.groups, w - 1);
         constexpr bool kFused =
             std::is_same<FL, PlainFlush<float>>::value && !COUNT;
         {
@@ -389,11 +392,11 @@ __device__ __forceinline__ void process_task(const TapVis<GT>* __restrict__ s_vi
             const TapVis<GT> v = s_vis[i0];
             const unsigned ru = min((unsigned)(a + v.mu),
                                     (unsigned)(a + v.mu - w));
+            const unsigned xb = (unsigned)(b0 + v.mv);
 #pragma unroll
             for (int q = 0; q < CPT; ++q)
             {
-                const unsigned rv = min((unsigned)(bq[q] + v.mv),
-                                        (unsigned)(bq[q] + v.mv - w));
+                const unsigned rv = min(xb + q, xb + q - (unsigned)w);
                 cur[q] = v.origin + ru + rv * (unsigned)grid_size;
                 acc[q].x = acc[q].y = GT(0);
             }
@@ -419,11 +422,11 @@ __device__ __forceinline__ void process_task(const TapVis<GT>* __restrict__ s_vi
             // are requested before any is used.
             unsigned rvs[CPT];
             typename KernelLoad<KT>::Wide kv[CPT];
+            const unsigned xb = (unsigned)(b0 + v.mv);
 #pragma unroll
             for (int q = 0; q < CPT; ++q)
             {
-                rvs[q] = min((unsigned)(bq[q] + v.mv),
-                             (unsigned)(bq[q] + v.mv - w));
+                rvs[q] = min(xb + q, xb + q - (unsigned)w);
                 kv[q] = KernelLoad<KT>::get(load_kernel<GMEM>(
                     reinterpret_cast<const KT*>(kp + (size_t)rvs[q] * pitch_b)));
             }
@@ -433,12 +436,12 @@ __device__ __forceinline__ void process_task(const TapVis<GT>* __restrict__ s_vi
                 const unsigned cell = cell0 + rvs[q] * (unsigned)grid_size;
                 if constexpr (kFused)
                 {
-                    flush.flush_reset(q < rows_here, cell, cur[q], acc[q].x,
+                    flush.flush_reset(q >= skip, cell, cur[q], acc[q].x,
                                       acc[q].y);
                 }
                 else
                 {
-                    const bool change = q < rows_here && cell != cur[q];
+                    const bool change = q >= skip && cell != cur[q];
                     flush(change, cur[q], acc[q].x, acc[q].y);
                     if (COUNT) flushes += change;
                     acc[q].x = change ? GT(0) : acc[q].x;
@@ -453,8 +456,8 @@ __device__ __forceinline__ void process_task(const TapVis<GT>* __restrict__ s_vi
         }
 #pragma unroll
         for (int q = 0; q < CPT; ++q)
-            flush(q < rows_here, cur[q], acc[q].x, acc[q].y);
-        if (COUNT) flushes += rows_here > 0 ? rows_here : 0;
+            flush(q >= skip, cur[q], acc[q].x, acc[q].y);
+        if (COUNT) flushes += CPT - skip;
     }
 }
 
@@ -468,6 +471,9 @@ __device__ __forceinline__ void dispatch_cpt(int cpt, const TapVis<GT>* s_vis,
 #define B200_CPT(C)                                                         \
     process_task<GT, KT, C, COUNT, GMEM, FL>(s_vis, m, w, pitch, row_shift, \
                                              slab, fl, grid_size, flushes)
+    // A row group never has more rows than the footprint (W = 1, 3, 5
+    // take CPT = W).
+    if (cpt > w) cpt = w;
     switch (cpt)
     {
     case 1: B200_CPT(1); break;
@@ -774,7 +780,8 @@ cudaError_t launch_variant(const GridArgs& a, int num_sms, size_t smem,
 // process_task: per visibility a thread does ~12 instructions of shared
 // column work plus ~20 per class, so the cost of a tap is
 // (12 / CPT + 20) / utilisation, utilisation being the fraction of the
-// CTA's thread slots holding a live class.
+// CTA's thread slots (threads x CPT x passes) holding a live class under
+// the (column, row group) layout of process_task.
 void default_tune_table(unsigned char* cpt)
 {
     const int choices[] = {1, 2, 3, 4, 5, 6};
@@ -785,21 +792,10 @@ void default_tune_table(unsigned char* cpt)
         int pick = 1;
         for (int c : choices)
         {
-            const int need = (w + c - 1) / c;
-            int groups, passes, slices;
-            if (w * need <= kGridThreads)
-            {
-                groups = need;
-                passes = 1;
-                slices = kGridThreads / (w * need);
-            }
-            else
-            {
-                groups = kGridThreads / w;
-                passes = (w + groups * c - 1) / (groups * c);
-                slices = 1;
-            }
-            (void)groups;
+            if (c > w) continue;
+            const int items = w * ((w + c - 1) / c);
+            const int slices = items <= kGridThreads ? kGridThreads / items : 1;
+            const int passes = (items + kGridThreads - 1) / kGridThreads;
             const double util = (double)w * w * slices /
                                 ((double)kGridThreads * c * passes);
             const double cost = (12.0 / c + 20.0) / util;
