@@ -413,7 +413,7 @@ def run_b200(args, world, rank, local):
                  "issued_atomic_frac": round(
                      issued_atomics / (kernel_ms * 1e-3) / rate.value, 4)}
     stage_ms = {"prep": round(stats.prep_ms, 3), "sort": round(stats.sort_ms, 3),
-                "permute_tasks": round(stats.tasks_ms, 3),
+                "tasks": round(stats.tasks_ms, 3),
                 "grid": round(stats.grid_ms, 3)}
 
     # End to end through the drop-in C entry point with pinned host buffers.
@@ -675,7 +675,7 @@ def run_batch128(args, world, rank, local):
             "grid_updates_per_s": st.grid_updates * world / (batch32_ms * 1e-3),
             "stage_ms": {"prep": round(st.prep_ms, 3),
                          "sort": round(st.sort_ms, 3),
-                         "permute_tasks": round(st.tasks_ms, 3),
+                         "tasks": round(st.tasks_ms, 3),
                          "grid": round(st.grid_ms, 3)},
             "gpu_launches": st.kernel_launches * args.steps,
             "rel_err_vs_fp64": err,

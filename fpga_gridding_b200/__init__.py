@@ -12,5 +12,6 @@ from .gridder import (Blocks, Cube, Workspace, degrid_device, degrid_host, grid_
                       options, oskar_grid_weights_read_d,
                       oskar_grid_weights_read_f, oskar_grid_weights_write_d,
                       oskar_grid_weights_write_f, oskar_grid_wproj_d,
-                      oskar_grid_wproj_f, place_device, weights_read_device,
+                      oskar_grid_wproj_f, oskar_grid_wproj_f_diagnostics,
+                      place_device, weights_read_device,
                       weights_write_device)

@@ -13,6 +13,7 @@ LIB_PATH = os.path.join(HERE, "libgridder_b200.so")
 EXPORTED_SYMBOLS = (
     "oskar_grid_wproj_d",
     "oskar_grid_wproj_f",
+    "oskar_grid_wproj_f_diagnostics",
     "oskar_grid_weights_write_d",
     "oskar_grid_weights_read_d",
     "oskar_grid_weights_write_f",
@@ -145,6 +146,9 @@ def load():
     lib.oskar_grid_wproj_f.argtypes = grid_common + [
         C.c_float, C.c_float, C.c_int, _P, _P, _P]
     lib.oskar_grid_wproj_d.restype = lib.oskar_grid_wproj_f.restype = None
+    lib.oskar_grid_wproj_f_diagnostics.argtypes = grid_common + [
+        C.c_float, C.c_float, C.c_int, _P, _P, _P, _P, _P, _P, _P, _P]
+    lib.oskar_grid_wproj_f_diagnostics.restype = None
     for t, real in (("d", C.c_double), ("f", C.c_float)):
         fw = getattr(lib, "oskar_grid_weights_write_" + t)
         fw.argtypes = [_SZ, _P, _P, _P, real, C.c_int, _P, _P]

@@ -11,6 +11,7 @@
 #include "band_rows.h"
 #include "ingest_plan.h"
 #include "common.cuh"
+#include "prep.cuh"
 #include "grid_romein.cuh"
 #include "internal.h"
 
@@ -576,7 +577,7 @@ size_t oskar_b200_workspace_bytes(const oskar_B200Workspace* ws)
     if (!ws) return 0;
     const DeviceBuffer* bufs[] = {
         &ws->keys[0], &ws->keys[1], &ws->vals[0], &ws->vals[1], &ws->rec,
-        &ws->srec, &ws->svis, &ws->scan_tmp, &ws->flags, &ws->task_start,
+        &ws->scan_tmp, &ws->flags, &ws->task_start, &ws->task_job,
         &ws->counters, &ws->partials, &ws->plane_counts, &ws->in_uu,
         &ws->in_vv, &ws->in_ww, &ws->in_vis, &ws->in_weight, &ws->in_grid,
         &ws->in_cube, &ws->in_norm, &ws->comp_grid};
@@ -1229,11 +1230,216 @@ int weights_read_drop_in(size_t n, const T* uu, const T* vv,
 
 #undef B200_PCHECK
 
+// oskar_grid_wproj_f_diagnostics on the caller's host arrays: the gridding
+// (grid, norm, skip count) as oskar_grid_wproj_f with the reference's float
+// coordinate arithmetic, then the hit counts (diagnostics.cu).  Histogram
+// sizes: num_vis_per_wsupport covers support values 0 .. max(support),
+// num_vis_per_wplane the unclamped plane indices of the points, as the
+// reference indexes them.  Every result goes back only after the device
+// work has succeeded.
+int diagnostics_drop_in(size_t num_w_planes, const int* support,
+                        int oversample, int conv_size_half,
+                        const float* conv_func, size_t n, const float* uu,
+                        const float* vv, const float* ww, const float* vis,
+                        float cell_size_rad, float w_scale, int grid_size,
+                        size_t* num_skipped, double* norm, float* grid,
+                        long long* num_vis_per_wsupport,
+                        long long* num_vis_per_wplane,
+                        long long* num_vis_per_grid,
+                        float* avg_wsupport_per_grid)
+{
+    if (!num_skipped || !norm || !grid || !num_vis_per_wsupport ||
+        !num_vis_per_wplane || !num_vis_per_grid || !avg_wsupport_per_grid)
+        return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    int st = validate_cube_args(num_w_planes, support, oversample,
+                                conv_size_half, conv_func);
+    if (st) return st;
+    st = check_grid_args(n, uu, vv, ww, vis, nullptr, 0, grid_size, grid);
+    if (st) return st;
+    oskar_B200Workspace* ws = nullptr;
+    st = dropin_workspace(&ws);
+    if (st) return st;
+    ThreadCache& tc = tls_cache;
+    if (!tc.cube)
+    {
+        tc.cube = new (std::nothrow) oskar_B200Cube();
+        if (!tc.cube) return OSKAR_B200_ERR_OUT_OF_MEMORY;
+    }
+    cudaStream_t s = ws->stream;
+#define B200_DCHECK(expr)                                           \
+    do {                                                            \
+        const cudaError_t e_ = (expr);                              \
+        if (e_ != cudaSuccess) { cudaStreamSynchronize(s);          \
+                                 cudaGetLastError();                \
+                                 return status_from_cuda(e_); }     \
+    } while (0)
+    const size_t G = (size_t)grid_size, cells = G * G;
+    const size_t cube_elems = num_w_planes * (size_t)conv_size_half *
+                              conv_size_half * 2;
+    int max_support = 0;
+    for (size_t p = 0; p < num_w_planes; ++p)
+        max_support = std::max(max_support, support[p]);
+    const size_t ns = (size_t)max_support + 1;
+    B200_DCHECK(ws->in_cube.ensure(cube_elems * sizeof(float)));
+    B200_DCHECK(ws->in_grid.ensure(2 * cells * sizeof(float)));
+    B200_DCHECK(ws->in_norm.ensure(8 * sizeof(unsigned long long)));
+    if (n)
+    {
+        B200_DCHECK(ws->in_uu.ensure(n * sizeof(float)));
+        B200_DCHECK(ws->in_vv.ensure(n * sizeof(float)));
+        B200_DCHECK(ws->in_ww.ensure(n * sizeof(float)));
+        B200_DCHECK(ws->in_vis.ensure(2 * n * sizeof(float)));
+    }
+    DeviceBuffer d_per_support, d_per_plane, d_per_cell, d_cell_sum;
+    B200_DCHECK(d_per_support.ensure(ns * sizeof(long long)));
+    B200_DCHECK(d_per_cell.ensure(cells * sizeof(long long)));
+    B200_DCHECK(d_cell_sum.ensure(cells * sizeof(float)));
+    const float* du = static_cast<const float*>(ws->in_uu.ptr);
+    const float* dv = static_cast<const float*>(ws->in_vv.ptr);
+    const float* dw = static_cast<const float*>(ws->in_ww.ptr);
+    unsigned long long* small =
+        static_cast<unsigned long long*>(ws->in_norm.ptr);
+    // small: [0] norm (double), [1] skip count, [2] device status,
+    // [3] largest unclamped plane, [4] unusable plane flag
+    B200_DCHECK(cudaMemcpyAsync(ws->in_cube.ptr, conv_func,
+                                cube_elems * sizeof(float),
+                                cudaMemcpyHostToDevice, s));
+    st = cube_init(tc.cube, ws->device, num_w_planes, support, oversample,
+                   conv_size_half, ws->in_cube.ptr, nullptr, 0, 0,
+                   OSKAR_B200_KERNEL_NATIVE, s);
+    if (st) { cudaStreamSynchronize(s); cudaGetLastError(); return st; }
+    if (n)
+    {
+        B200_DCHECK(cudaMemcpyAsync(ws->in_uu.ptr, uu, n * sizeof(float),
+                                    cudaMemcpyHostToDevice, s));
+        B200_DCHECK(cudaMemcpyAsync(ws->in_vv.ptr, vv, n * sizeof(float),
+                                    cudaMemcpyHostToDevice, s));
+        B200_DCHECK(cudaMemcpyAsync(ws->in_ww.ptr, ww, n * sizeof(float),
+                                    cudaMemcpyHostToDevice, s));
+        B200_DCHECK(cudaMemcpyAsync(ws->in_vis.ptr, vis,
+                                    2 * n * sizeof(float),
+                                    cudaMemcpyHostToDevice, s));
+    }
+    // The largest unclamped plane index sizes num_vis_per_wplane.
+    const float w_scale_f = w_scale;
+    B200_DCHECK(launch_diag_max_plane(dw, n, w_scale_f, small + 3,
+                                      ws->num_sms, s));
+    unsigned long long plane_info[2] = {0, 0};
+    B200_DCHECK(cudaMemcpyAsync(plane_info, small + 3, sizeof(plane_info),
+                                cudaMemcpyDeviceToHost, s));
+    B200_DCHECK(cudaStreamSynchronize(s));
+    if (plane_info[1]) return OSKAR_B200_ERR_INVALID_ARGUMENT;
+    const size_t np = n ? (size_t)plane_info[0] + 1 : 0;
+    if (np) B200_DCHECK(d_per_plane.ensure(np * sizeof(long long)));
+    // The caller's arrays accumulate: their current contents go up.
+    B200_DCHECK(cudaMemcpyAsync(ws->in_grid.ptr, grid,
+                                2 * cells * sizeof(float),
+                                cudaMemcpyHostToDevice, s));
+    B200_DCHECK(cudaMemcpyAsync(d_per_support.ptr, num_vis_per_wsupport,
+                                ns * sizeof(long long),
+                                cudaMemcpyHostToDevice, s));
+    if (np)
+        B200_DCHECK(cudaMemcpyAsync(d_per_plane.ptr, num_vis_per_wplane,
+                                    np * sizeof(long long),
+                                    cudaMemcpyHostToDevice, s));
+    B200_DCHECK(cudaMemcpyAsync(d_per_cell.ptr, num_vis_per_grid,
+                                cells * sizeof(long long),
+                                cudaMemcpyHostToDevice, s));
+    B200_DCHECK(cudaMemcpyAsync(d_cell_sum.ptr, avg_wsupport_per_grid,
+                                cells * sizeof(float),
+                                cudaMemcpyHostToDevice, s));
+    B200_DCHECK(cudaMemsetAsync(small, 0, 3 * sizeof(unsigned long long),
+                                s));
+    double* d_norm = reinterpret_cast<double*>(small);
+    oskar_B200Options opt;
+    oskar_b200_options_init(&opt);
+    opt.coord_mode = OSKAR_B200_COORDS_REFERENCE_F32;
+    HostJob j{};
+    j.cube = tc.cube;
+    j.num_points = n;
+    j.uu = du;
+    j.vv = dv;
+    j.ww = dw;
+    j.vis = ws->in_vis.ptr;
+    j.cell_size_rad = cell_size_rad;
+    j.w_scale = w_scale;
+    j.grid_size = grid_size;
+    j.grid = ws->in_grid.ptr;
+    j.d_num_skipped = small + 1;
+    j.d_norm = d_norm;
+    st = run_batch(ws, &opt, 1, &j, s, false, nullptr);
+    if (st) { cudaStreamSynchronize(s); cudaGetLastError(); return st; }
+    B200_DCHECK(launch_status_or(ws, small + 2, s));
+    PlaceConsts pc{};
+    pc.grid_scale = (double)grid_size * (double)cell_size_rad;
+    pc.w_scale = w_scale;
+    pc.grid_scale_f = (float)grid_size * cell_size_rad;
+    pc.w_scale_f = w_scale_f;
+    pc.grid_size = grid_size;
+    pc.centre = grid_size / 2;
+    pc.num_planes = (int)num_w_planes;
+    pc.oversample = oversample;
+    B200_DCHECK(launch_diag_counts(
+        du, dv, dw, n, pc, static_cast<const int*>(tc.cube->d_support.ptr),
+        static_cast<unsigned long long*>(d_per_support.ptr),
+        static_cast<unsigned long long*>(d_per_plane.ptr),
+        static_cast<unsigned long long*>(d_per_cell.ptr),
+        static_cast<float*>(d_cell_sum.ptr), ws->num_sms, s));
+    unsigned long long res[3];
+    B200_DCHECK(cudaMemcpyAsync(res, small, sizeof(res),
+                                cudaMemcpyDeviceToHost, s));
+    B200_DCHECK(cudaStreamSynchronize(s));
+    if (res[2]) return res[2] & DEV_ERR_TIMEOUT ? OSKAR_B200_ERR_TIMEOUT
+                                                : OSKAR_B200_ERR_DEVICE_CHECK;
+    B200_DCHECK(cudaMemcpyAsync(grid, ws->in_grid.ptr,
+                                2 * cells * sizeof(float),
+                                cudaMemcpyDeviceToHost, s));
+    B200_DCHECK(cudaMemcpyAsync(num_vis_per_wsupport, d_per_support.ptr,
+                                ns * sizeof(long long),
+                                cudaMemcpyDeviceToHost, s));
+    if (np)
+        B200_DCHECK(cudaMemcpyAsync(num_vis_per_wplane, d_per_plane.ptr,
+                                    np * sizeof(long long),
+                                    cudaMemcpyDeviceToHost, s));
+    B200_DCHECK(cudaMemcpyAsync(num_vis_per_grid, d_per_cell.ptr,
+                                cells * sizeof(long long),
+                                cudaMemcpyDeviceToHost, s));
+    B200_DCHECK(cudaMemcpyAsync(avg_wsupport_per_grid, d_cell_sum.ptr,
+                                cells * sizeof(float),
+                                cudaMemcpyDeviceToHost, s));
+    B200_DCHECK(cudaStreamSynchronize(s));
+#undef B200_DCHECK
+    double nrm;
+    memcpy(&nrm, &res[0], sizeof(nrm));
+    *norm += nrm;
+    *num_skipped = (size_t)res[1];
+    return OSKAR_B200_OK;
+}
+
 #undef B200_WCHECK
 
 }  // namespace
 
 extern "C" {
+
+void oskar_grid_wproj_f_diagnostics(const size_t num_w_planes,
+        const int* support, const int oversample, const int conv_size_half,
+        const float* conv_func, const size_t num_points, const float* uu,
+        const float* vv, const float* ww, const float* vis,
+        const float* weight, const float cell_size_rad, const float w_scale,
+        const int grid_size, size_t* num_skipped, double* norm, float* grid,
+        long long int* num_vis_per_wsupport, long long int* num_vis_per_wplane,
+        long long int* num_vis_per_grid, float* avg_wsupport_per_grid,
+        float* avg_wplane_per_grid)
+{
+    (void)weight;               // ignored, as in oskar_grid_wproj.c:299-300
+    (void)avg_wplane_per_grid;  // never written by the reference either
+    tls_status = diagnostics_drop_in(
+        num_w_planes, support, oversample, conv_size_half, conv_func,
+        num_points, uu, vv, ww, vis, cell_size_rad, w_scale, grid_size,
+        num_skipped, norm, grid, num_vis_per_wsupport, num_vis_per_wplane,
+        num_vis_per_grid, avg_wsupport_per_grid);
+}
 
 void oskar_grid_weights_write_d(const size_t num_points, const double* uu,
                                 const double* vv, const double* weight,

@@ -18,8 +18,9 @@ constexpr int kMaxOffsets = 33;     // 2 * ceil(oversample / 2) + 1, oversample 
 
 struct GridArgs
 {
-    const int4* srec;           // sorted placement records
-    const void* svis;           // sorted visibilities (float2 / double2)
+    const uint32_t* order;      // sorted position -> point (global index)
+    const int4* rec;            // placement record of each point
+    int apply_weight;           // visibilities x weight (see JobDesc)
     const uint32_t* task_start; // [num_tasks + 1]
     const uint32_t* task_job;   // [num_tasks]: job of each task
     const JobDesc* jobs;        // cube, grid and geometry of each job

@@ -124,7 +124,7 @@ struct oskar_B200Workspace
     size_t smem_optin = 0;
     cudaStream_t stream = nullptr;
     // per-visibility work arrays
-    b200::DeviceBuffer keys[2], vals[2], rec, srec, svis, scan_tmp, flags;
+    b200::DeviceBuffer keys[2], vals[2], rec, scan_tmp, flags;
     b200::DeviceBuffer task_start, task_job;
     // small arrays: counters, partial sums, per-job plane histograms and
     // skip counts, the job table

@@ -1,9 +1,10 @@
 // Gridding of a batch of jobs on device-resident data:
 //   prep (placement, keys, norms, skip counts, plane histograms)
 //   -> one radix sort of (key, index) over all jobs (job in the top bits)
-//   -> permute records and visibilities into sorted order
 //   -> task list (tasks never cross a job, tile or plane)
-//   -> one persistent Romein gridding launch over every task of every job.
+//   -> one persistent Romein gridding launch over every task of every job;
+//      each task gathers its points' records and visibilities through the
+//      sorted index (no separate permutation pass).
 // A single oskar_b200_grid call is a batch of one job.
 #include <algorithm>
 #include <atomic>
@@ -92,7 +93,6 @@ int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
         return OSKAR_B200_ERR_INVALID_ARGUMENT;
     const oskar_B200Cube* c0 = jobs[0].cube;
     const bool dbl = c0->data_is_double != 0;
-    const size_t vsz = dbl ? sizeof(double) : sizeof(float);
     const bool comp = !degrid &&
                       opt->accum_mode == OSKAR_B200_ACCUM_COMPENSATED;
     int launches = 0;
@@ -263,8 +263,6 @@ int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
         B200_TRY(ws->rec.ensure(16 * n));
         if (!degrid)
         {
-            B200_TRY(ws->srec.ensure(16 * n));
-            B200_TRY(ws->svis.ensure(2 * vsz * n));
             B200_TRY(ws->flags.ensure(4 * n));
             B200_TRY(ws->task_start.ensure(4 * (n + 2)));
             B200_TRY(ws->task_job.ensure(4 * (n + 2)));
@@ -341,11 +339,6 @@ int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
                                  cudaMemcpyDeviceToHost, st));
         return OSKAR_B200_OK;
     }
-    B200_TRY(launch_permute(vals[which], keys[which], n, counters, pa.rec,
-                            d_jobs, kl.job_shift, opt->apply_weight, dbl,
-                            static_cast<int4*>(ws->srec.ptr), ws->svis.ptr,
-                            ws->num_sms, st));
-    launches += 1;
     B200_TRY(launch_tasks(keys[which], n, counters, 2 * kl.fine_bits,
                           kl.job_shift, kTaskMax,
                           static_cast<uint32_t*>(ws->flags.ptr),
@@ -355,8 +348,9 @@ int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
                           ws->num_sms, st, &launches));
 
     GridArgs ga{};
-    ga.srec = static_cast<const int4*>(ws->srec.ptr);
-    ga.svis = ws->svis.ptr;
+    ga.order = vals[which];
+    ga.rec = pa.rec;
+    ga.apply_weight = opt->apply_weight;
     ga.task_start = static_cast<const uint32_t*>(ws->task_start.ptr);
     ga.task_job = static_cast<const uint32_t*>(ws->task_job.ptr);
     ga.jobs = d_jobs;

@@ -247,41 +247,6 @@ __global__ void finalize_prep_kernel(const PrepArgs a)
     }
 }
 
-// One position per thread per step.  (Four per thread, their gathers
-// issued together, measured 1.57 -> 1.52 ms at plain_large but stalled the
-// server's mixed stream: p50 latency 4.9 -> 28-135 ms at 340 jobs/s, so
-// the plain loop stays.)
-template <typename T>
-__global__ void permute_kernel(const uint32_t* __restrict__ order,
-                               const uint32_t* __restrict__ sorted_keys,
-                               size_t n,
-                               const unsigned long long* __restrict__ counters,
-                               const int4* __restrict__ rec,
-                               const JobDesc* __restrict__ jobs, int job_shift,
-                               int apply_weight, int4* __restrict__ srec,
-                               T* __restrict__ svis)
-{
-    const size_t valid = n - counters[CNT_SKIPPED];
-    for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < valid;
-         s += (size_t)gridDim.x * blockDim.x)
-    {
-        const uint32_t i = order[s];
-        const JobDesc& jd = jobs[sorted_keys[s] >> job_shift];
-        const size_t local = i - jd.first;
-        const T* vis = static_cast<const T*>(jd.vis);
-        srec[s] = rec[i];
-        T re = vis[2 * local], im = vis[2 * local + 1];
-        if (apply_weight)
-        {
-            const T w = static_cast<const T*>(jd.weight)[local];
-            re *= w;
-            im *= w;
-        }
-        svis[2 * s] = re;
-        svis[2 * s + 1] = im;
-    }
-}
-
 __global__ void task_flags_kernel(const uint32_t* __restrict__ keys, size_t n,
                                   const unsigned long long* __restrict__ counters,
                                   int fine_key_bits, int task_max,
@@ -374,24 +339,6 @@ cudaError_t launch_prep(const PrepArgs& a, int data_is_double, int coord_mode,
 cudaError_t launch_finalize_prep(const PrepArgs& a, cudaStream_t st)
 {
     finalize_prep_kernel<<<a.num_jobs, 256, 0, st>>>(a);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_permute(const uint32_t* order, const uint32_t* sorted_keys,
-                           size_t n, const unsigned long long* counters,
-                           const int4* rec, const JobDesc* jobs, int job_shift,
-                           int apply_weight, int data_is_double, int4* srec,
-                           void* svis, int num_sms, cudaStream_t st)
-{
-    const unsigned blocks = grid_blocks(n, num_sms, 8, 256);
-    if (data_is_double)
-        permute_kernel<double><<<blocks, 256, 0, st>>>(
-            order, sorted_keys, n, counters, rec, jobs, job_shift,
-            apply_weight, srec, static_cast<double*>(svis));
-    else
-        permute_kernel<float><<<blocks, 256, 0, st>>>(
-            order, sorted_keys, n, counters, rec, jobs, job_shift,
-            apply_weight, srec, static_cast<float*>(svis));
     return cudaGetLastError();
 }
 

@@ -140,12 +140,6 @@ cudaError_t launch_prep(const PrepArgs& a, int data_is_double, int coord_mode,
                         cudaStream_t st);
 // Per job: norm += sum of its partials; skip count; grid updates.
 cudaError_t launch_finalize_prep(const PrepArgs& a, cudaStream_t st);
-// srec[s] = rec[order[s]], svis[s] = vis of that point (x weight).
-cudaError_t launch_permute(const uint32_t* order, const uint32_t* sorted_keys,
-                           size_t n, const unsigned long long* counters,
-                           const int4* rec, const JobDesc* jobs, int job_shift,
-                           int apply_weight, int data_is_double, int4* srec,
-                           void* svis, int num_sms, cudaStream_t st);
 // Task list: a task starts where (job, coarse tile, plane) changes and every
 // task_max positions; task_job[t] is the job of task t.
 cudaError_t launch_tasks(const uint32_t* sorted_keys, size_t n,
@@ -162,6 +156,23 @@ cudaError_t launch_band_first(const uint32_t* sorted_keys,
                               const KeyLayout& kl, int num_bands,
                               uint32_t* band_first, int num_sms,
                               cudaStream_t st);
+// oskar_grid_wproj_f_diagnostics (diagnostics.cu).  Unclamped w-plane
+// indices at or above kDiagMaxPlanes are refused.
+constexpr unsigned kDiagMaxPlanes = 1u << 24;
+// out[0] = the largest unclamped w-plane index of the points, out[1] = 1
+// when any index is not finite or not below kDiagMaxPlanes.
+cudaError_t launch_diag_max_plane(const float* ww, size_t n, float w_scale_f,
+                                  unsigned long long* out, int num_sms,
+                                  cudaStream_t st);
+// The per-support, per-plane and per-cell counts and the per-cell support +
+// plane sums of the diagnostics gridder, with its float placement.
+cudaError_t launch_diag_counts(const float* uu, const float* vv,
+                               const float* ww, size_t n,
+                               const PlaceConsts& pc, const int* support,
+                               unsigned long long* per_support,
+                               unsigned long long* per_plane,
+                               unsigned long long* per_cell, float* cell_sum,
+                               int num_sms, cudaStream_t st);
 cudaError_t launch_place(int data_is_double, int coord_mode, const void* uu,
                          const void* vv, const void* ww, size_t n,
                          const PlaceConsts& pc, const int* support,

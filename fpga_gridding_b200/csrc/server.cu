@@ -75,9 +75,11 @@ struct Slot
 };
 
 // Workspace bytes a batch of n points needs (run_batch's buffers).
-size_t workspace_need(size_t n, bool dbl)
+size_t workspace_need(size_t n)
 {
-    return n * (dbl ? 80u : 72u) + (8u << 20);
+    // keys and indices (twice), records, task flags, starts and jobs, and
+    // the sort's scratch: 48 bytes per point in either precision
+    return n * 48u + (8u << 20);
 }
 
 }  // namespace
@@ -219,8 +221,7 @@ struct oskar_B200Server
                     break;
                 }
                 if (!pick.empty() && n + p.req.num_points > kBatchPoints) break;
-                const bool dbl = p.req.cube->data_is_double != 0;
-                const size_t ws_need = workspace_need(n + p.req.num_points, dbl);
+                const size_t ws_need = workspace_need(n + p.req.num_points);
                 const size_t grow = ws_need > have ? ws_need - have : 0;
                 trim_pool(grow + gbytes + p.grid_bytes);
                 if (in_use() + grow + gbytes + p.grid_bytes > budget) break;

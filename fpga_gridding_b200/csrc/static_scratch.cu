@@ -39,7 +39,7 @@ int static_cube_fill(const float* d_conv, int num_planes, int oversample,
 
 namespace {
 
-// 64 MiB: about 850,000 visibilities with a small cube (~73 bytes of
+// 64 MiB: about 1.4 million visibilities with a small cube (~45 bytes of
 // scratch per visibility plus the re-laid cube).
 constexpr size_t kStaticScratchBytes = size_t(64) << 20;
 constexpr int kMaxDevices = 64;
@@ -149,8 +149,6 @@ extern "C" int oskar_b200_grid_f_static(
     uint32_t* keys[2] = {cv.take<uint32_t>(4 * n), cv.take<uint32_t>(4 * n)};
     uint32_t* vals[2] = {cv.take<uint32_t>(4 * n), cv.take<uint32_t>(4 * n)};
     auto* rec = cv.take<int4>(16 * n);
-    auto* srec = cv.take<int4>(16 * n);
-    auto* svis = cv.take<float>(8 * n);
     auto* flags = cv.take<uint32_t>(4 * n);
     auto* task_start = cv.take<uint32_t>(4 * (n + 2));
     auto* task_job = cv.take<uint32_t>(4 * (n + 2));
@@ -234,14 +232,13 @@ extern "C" int oskar_b200_grid_f_static(
     int which = 0;
     B200_S(radix_sort_pairs(keys, vals, n, kl.total_bits + 1, scan_tmp, s,
                             &which, nullptr));
-    B200_S(launch_permute(vals[which], keys[which], n, counters, rec, d_job,
-                          kl.job_shift, 0, 0, srec, svis, num_sms, s));
     B200_S(launch_tasks(keys[which], n, counters, 2 * kl.fine_bits,
                         kl.job_shift, kTaskMax, flags, keys[which ^ 1],
                         scan_tmp, task_start, task_job, num_sms, s, nullptr));
     GridArgs ga{};
-    ga.srec = srec;
-    ga.svis = svis;
+    ga.order = vals[which];
+    ga.rec = rec;
+    ga.apply_weight = 0;
     ga.task_start = task_start;
     ga.task_job = task_job;
     ga.jobs = d_job;

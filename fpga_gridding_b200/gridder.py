@@ -66,6 +66,36 @@ def oskar_grid_wproj_f(num_w_planes, support, oversample, conv_size_half,
                    w_scale, grid_size, norm, grid)
 
 
+def oskar_grid_wproj_f_diagnostics(num_w_planes, support, oversample,
+                                   conv_size_half, conv_func, num_points, uu,
+                                   vv, ww, vis, weight, cell_size_rad,
+                                   w_scale, grid_size, norm, grid,
+                                   num_vis_per_wsupport, num_vis_per_wplane,
+                                   num_vis_per_grid, avg_wsupport_per_grid,
+                                   avg_wplane_per_grid):
+    """oskar_grid_wproj.c:245-370 on the GPU: the float-coordinate FP32
+    gridder plus hit counts.  The grid (float32), the int64 count arrays and
+    avg_wsupport_per_grid (float32) accumulate in place; returns
+    (num_skipped, norm)."""
+    lib = load()
+    support = np.ascontiguousarray(support, dtype=np.int32)
+    skipped = C.c_size_t(0)
+    nrm = C.c_double(norm)
+    fn = lib.oskar_grid_wproj_f_diagnostics
+    fn(num_w_planes, _carr(support, np.int32), oversample, conv_size_half,
+       _carr(conv_func, np.float32), num_points, _carr(uu, np.float32),
+       _carr(vv, np.float32), _carr(ww, np.float32), _carr(vis, np.float32),
+       _carr(weight, np.float32) if weight is not None else None,
+       cell_size_rad, w_scale, grid_size, C.byref(skipped), C.byref(nrm),
+       _carr(grid, np.float32), _carr(num_vis_per_wsupport, np.int64),
+       _carr(num_vis_per_wplane, np.int64), _carr(num_vis_per_grid, np.int64),
+       _carr(avg_wsupport_per_grid, np.float32),
+       _carr(avg_wplane_per_grid, np.float32)
+       if avg_wplane_per_grid is not None else None)
+    check(lib.oskar_grid_wproj_b200_last_error(), fn.__name__)
+    return skipped.value, nrm.value
+
+
 def grid_workload(w: dict, single: bool, grid=None, norm: float = 0.0):
     """Drop-in call on a Workload.numpy() dict.  Returns
     (num_skipped, norm, grid)."""

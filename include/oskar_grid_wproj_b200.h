@@ -106,6 +106,51 @@ void oskar_grid_wproj_f(
         double* norm,
         float* grid);
 
+/* Replaces oskar_grid_wproj_f_diagnostics (oskar_grid_wproj.c:245-370;
+ * defined there, declared in no reference header): oskar_grid_wproj_f over
+ * all num_points with the reference's float coordinate arithmetic, plus hit
+ * counts, all accumulating into the caller's arrays:
+ *   num_vis_per_wsupport[w_support] += 1 and num_vis_per_wplane[grid_w] += 1
+ *     for every point, skipped or not, where grid_w =
+ *     round(sqrt(|w * w_scale|)) before it is clamped to the last plane and
+ *     w_support is the support of the plane actually used;
+ *   for every tap of a kept point, at its grid cell (grid_size^2 arrays,
+ *     row-major in v): num_vis_per_grid += 1, avg_wsupport_per_grid +=
+ *     w_support + grid_w (both into the same array, as the reference
+ *     does); avg_wplane_per_grid is never written.
+ * num_vis_per_wsupport must hold max(support) + 1 entries and
+ * num_vis_per_wplane the largest grid_w of the points + 1, as the
+ * reference's indexing requires; a point whose grid_w is not finite or not
+ * below 2^24 fails the call with OSKAR_B200_ERR_INVALID_ARGUMENT.  Counts
+ * are exact; the per-cell sums are exact while they stay below 2^24 (the
+ * reference's own float sums round beyond that).  Synchronous; on failure
+ * the outputs are untouched and the status is available from
+ * oskar_grid_wproj_b200_last_error(). */
+OSKAR_B200_EXPORT
+void oskar_grid_wproj_f_diagnostics(
+        const size_t num_w_planes,
+        const int* support,
+        const int oversample,
+        const int conv_size_half,
+        const float* conv_func,
+        const size_t num_points,
+        const float* uu,
+        const float* vv,
+        const float* ww,
+        const float* vis,
+        const float* weight,
+        const float cell_size_rad,
+        const float w_scale,
+        const int grid_size,
+        size_t* num_skipped,
+        double* norm,
+        float* grid,
+        long long int* num_vis_per_wsupport,
+        long long int* num_vis_per_wplane,
+        long long int* num_vis_per_grid,
+        float* avg_wsupport_per_grid,
+        float* avg_wplane_per_grid);
+
 /* Replace oskar_grid_weights_{write,read}_{d,f} (utils/oskar_grid_weights.h:
  * 60-65, 84-89, 107-112, 131-136): the "uniform" weighting histogram and its
  * density lookup, computed on the GPU on the caller's host arrays.  Same
@@ -395,7 +440,7 @@ typedef struct oskar_B200Stats
     int kernel_launches;               /* kernels the call launched */
     /* Stage durations in ms (CUDA events on the call's stream), filled
      * when stage timing is enabled on the workspace, else 0: placement and
-     * keys, radix sort, permutation and task list, gridding kernel. */
+     * keys, radix sort, task list, gridding kernel. */
     float prep_ms, sort_ms, tasks_ms, grid_ms;
 } oskar_B200Stats;
 
@@ -474,7 +519,7 @@ OSKAR_B200_EXPORT int oskar_b200_measure_atomic_rate(oskar_B200Workspace* ws,
  * are device pointers; support is host memory; weight is ignored as in the
  * reference.  All scratch (the re-laid cube, sort keys, records, task list)
  * comes from one static device array of 64 MiB that every GPU loading this
- * library holds until the process exits: enough for about 850,000
+ * library holds until the process exits: enough for about 1.4 million
  * visibilities with a small cube.  A job that does not fit returns
  * OSKAR_B200_ERR_OVER_BUDGET and touches nothing.  The array's device
  * address is looked up on the first call on each device (with that device

@@ -255,6 +255,70 @@ void orc_grid_wproj_f(size_t num_w_planes, const int* support, int oversample,
     }
 }
 
+/* oskar_grid_wproj_f_diagnostics, oskar_grid_wproj.c:245-370: the float
+ * gridder of oskar_grid_wproj_f over all num_points, plus hit counts.  For
+ * every point (skipped or not), with grid_w = round(sqrt(|w * w_scale|))
+ * before clamping and w_support the support of the clamped plane:
+ *   num_vis_per_wsupport[w_support] += 1, num_vis_per_wplane[grid_w] += 1
+ * (:317-318); for every tap of a kept point, at its grid cell:
+ *   num_vis_per_grid += 1, avg_wsupport_per_grid += w_support, then
+ *   avg_wsupport_per_grid += grid_w (:358-360: both sums go to the same
+ *   array); avg_wplane_per_grid is never written. */
+void orc_grid_wproj_f_diagnostics(size_t num_w_planes, const int* support,
+        int oversample, int conv_size_half, const float* conv_func,
+        size_t num_points, const float* uu, const float* vv,
+        const float* ww, const float* vis, const float* weight,
+        float cell_size_rad, float w_scale, int grid_size,
+        size_t* num_skipped, double* norm, float* grid,
+        long long* num_vis_per_wsupport, long long* num_vis_per_wplane,
+        long long* num_vis_per_grid, float* avg_wsupport_per_grid,
+        float* avg_wplane_per_grid)
+{
+    const size_t plane_elems = (size_t)conv_size_half * conv_size_half;
+    const float grid_scale = grid_size * cell_size_rad;
+    size_t n;
+    (void)weight;
+    (void)avg_wplane_per_grid;
+    *num_skipped = 0;
+    for (n = 0; n < num_points; ++n)
+    {
+        Place p;
+        double tap_sum = 0.0;
+        int dv, du;
+        place_f(num_w_planes, support, oversample, grid_scale, grid_size,
+                w_scale, uu[n], vv[n], ww[n], &p);
+        num_vis_per_wsupport[p.support] += 1;
+        num_vis_per_wplane[p.raw_plane] += 1;
+        if (p.skipped) { *num_skipped += 1; continue; }
+        {
+            const float a_re = vis[2 * n], a_im = vis[2 * n + 1];
+            const float sgn = (float)p.conj;
+            const size_t plane_base = p.plane * plane_elems;
+            for (dv = -p.support; dv <= p.support; ++dv)
+            {
+                const size_t row = (size_t)(p.gv + dv) * (size_t)grid_size;
+                const size_t krow = plane_base + (size_t)abs(p.off_v +
+                        dv * oversample) * (size_t)conv_size_half;
+                for (du = -p.support; du <= p.support; ++du)
+                {
+                    const size_t ki = 2 * (krow +
+                            (size_t)abs(p.off_u + du * oversample));
+                    const size_t cell = row + (size_t)(p.gu + du);
+                    const float k_re = conv_func[ki];
+                    const float k_im = conv_func[ki + 1] * sgn;
+                    grid[2 * cell]     += (a_re * k_re - a_im * k_im);
+                    grid[2 * cell + 1] += (a_im * k_re + a_re * k_im);
+                    num_vis_per_grid[cell] += 1;
+                    avg_wsupport_per_grid[cell] += (float)p.support;
+                    avg_wsupport_per_grid[cell] += (float)p.raw_plane;
+                    tap_sum += k_re;
+                }
+            }
+        }
+        *norm += tap_sum;
+    }
+}
+
 /* ------------------------------------------------------------------ */
 /* Placement tuples.                                                    */
 /* ------------------------------------------------------------------ */

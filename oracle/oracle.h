@@ -55,6 +55,21 @@ void orc_grid_wproj_f(size_t num_w_planes, const int* support, int oversample,
         float w_scale, int grid_size, size_t* num_skipped, double* norm,
         float* grid);
 
+/* Restates oskar_grid_wproj_f_diagnostics, oskar_grid_wproj.c:245-370:
+ * oskar_grid_wproj_f's float gridding of all num_points plus per-support,
+ * per-plane (unclamped) and per-cell hit counts and the per-cell sum of
+ * support + plane of every tap (in avg_wsupport_per_grid, as the reference
+ * writes it; avg_wplane_per_grid is not touched). */
+void orc_grid_wproj_f_diagnostics(size_t num_w_planes, const int* support,
+        int oversample, int conv_size_half, const float* conv_func,
+        size_t num_points, const float* uu, const float* vv,
+        const float* ww, const float* vis, const float* weight,
+        float cell_size_rad, float w_scale, int grid_size,
+        size_t* num_skipped, double* norm, float* grid,
+        long long* num_vis_per_wsupport, long long* num_vis_per_wplane,
+        long long* num_vis_per_grid, float* avg_wsupport_per_grid,
+        float* avg_wplane_per_grid);
+
 /* Per-visibility placement tuple, FP64 coordinate arithmetic of
  * oskar_grid_wproj.c:70-101.  plane is the clamped w-plane actually used
  * (min(grid_w, num_w_planes-1)); raw_plane is grid_w before clamping

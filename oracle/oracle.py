@@ -34,6 +34,7 @@ _GRID_ARGS_D = [_SZ, _P, C.c_int, C.c_int, _P, _SZ, _P, _P, _P, _P, _P,
                 C.c_double, C.c_double, C.c_int, _P, _P, _P]
 _GRID_ARGS_F = [_SZ, _P, C.c_int, C.c_int, _P, _SZ, _P, _P, _P, _P, _P,
                 C.c_float, C.c_float, C.c_int, _P, _P, _P]
+_DIAG_ARGS = _GRID_ARGS_F + [_P] * 5
 GRID_FN_D = C.CFUNCTYPE(None, *_GRID_ARGS_D)
 GRID_FN_F = C.CFUNCTYPE(None, *_GRID_ARGS_F)
 
@@ -98,6 +99,8 @@ def oracle_lib():
         lib.orc_degrid_wproj_d.restype = None
         lib.orc_scale_coords.argtypes = [C.c_double, C.c_int, _SZ, _P, _P, _P]
         lib.orc_scale_coords.restype = None
+        lib.orc_grid_wproj_f_diagnostics.argtypes = _DIAG_ARGS
+        lib.orc_grid_wproj_f_diagnostics.restype = None
         _oracle = lib
     return _oracle
 
@@ -115,6 +118,8 @@ def reference_lib():
             r = getattr(lib, "ref_oskar_grid_weights_read_" + t)
             r.argtypes = [_SZ, _P, _P, _P, _P, real, C.c_int, _P, _P]
             w.restype = r.restype = None
+        lib.ref_oskar_grid_wproj_f_diagnostics.argtypes = _DIAG_ARGS
+        lib.ref_oskar_grid_wproj_f_diagnostics.restype = None
         _ref = lib
     return _ref
 
@@ -208,6 +213,55 @@ def grid_f(w, grid_arr=None, norm=0.0, threads=None):
     lib = oracle_lib()
     fn = lib.orc_grid_wproj_f if threads is None else lib.orc_grid_wproj_f_banded
     return grid(fn, w, np.float32, grid_arr, norm, threads)
+
+
+def diagnostics_sizes(w: dict):
+    """Entries the diagnostics histograms need: (max support + 1, largest
+    unclamped w-plane index of the points + 1), with the reference's float
+    arithmetic."""
+    p = place(w, single=True)
+    return (int(np.max(w["support"])) + 1,
+            int(p["raw_plane"].astype(np.int64).max(initial=0)) + 1)
+
+
+def diagnostics_f(w: dict, use_reference: bool = False, init=None):
+    """oskar_grid_wproj_f_diagnostics (restated, or the reference's own) on
+    the arrays of `w`.  `init` optionally gives the starting contents of the
+    in/out arrays (grid, norm, num_vis_per_wsupport, num_vis_per_wplane,
+    num_vis_per_grid, avg_wsupport_per_grid, avg_wplane_per_grid); returns
+    a dict of them and num_skipped."""
+    a = _arrays(w, np.float32)
+    g = w["grid_size"]
+    ns, npl = diagnostics_sizes(w)
+    out = dict(grid=np.zeros(2 * g * g, np.float32), norm=0.0,
+               num_vis_per_wsupport=np.zeros(ns, np.int64),
+               num_vis_per_wplane=np.zeros(npl, np.int64),
+               num_vis_per_grid=np.zeros(g * g, np.int64),
+               avg_wsupport_per_grid=np.zeros(g * g, np.float32),
+               avg_wplane_per_grid=np.zeros(g * g, np.float32))
+    if init:
+        for k, v in init.items():
+            out[k] = v if k == "norm" else np.array(v, copy=True)
+    if use_reference:
+        lib = reference_lib()
+        if lib is None:
+            raise RuntimeError("reference library not built")
+        fn = lib.ref_oskar_grid_wproj_f_diagnostics
+    else:
+        fn = oracle_lib().orc_grid_wproj_f_diagnostics
+    skipped = C.c_size_t(0)
+    nrm = C.c_double(out["norm"])
+    fn(w["num_w_planes"], _ptr(a["support"]), w["oversample"],
+       w["conv_size_half"], _ptr(a["conv_func"]), a["uu"].shape[0],
+       _ptr(a["uu"]), _ptr(a["vv"]), _ptr(a["ww"]), _ptr(a["vis"]),
+       _ptr(a["weight"]), w["cell_size_rad"], w["w_scale"], g,
+       C.byref(skipped), C.byref(nrm), _ptr(out["grid"]),
+       _ptr(out["num_vis_per_wsupport"]), _ptr(out["num_vis_per_wplane"]),
+       _ptr(out["num_vis_per_grid"]), _ptr(out["avg_wsupport_per_grid"]),
+       _ptr(out["avg_wplane_per_grid"]))
+    out["norm"] = nrm.value
+    out["num_skipped"] = skipped.value
+    return out
 
 
 def place(w: dict, single: bool = False):

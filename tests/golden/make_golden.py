@@ -208,6 +208,47 @@ def save(name, inputs, single):
     print(f"{name}: n={len(inputs['uu'])} skipped={skipped} norm={norm:.17g}")
 
 
+def save_diagnostics(name, inputs, seed=17):
+    """Runs the reference's oskar_grid_wproj_f_diagnostics on the inputs
+    (as float) with every in/out array starting from random contents (the
+    counts and per-cell sums from small integers, so the accumulation stays
+    exact; the plane histogram random over its first 64 entries, zero
+    beyond) and stores inputs, starting contents and outputs."""
+    rng = np.random.default_rng(seed)
+    w = dict(inputs)
+    for k in ("conv_func", "uu", "vv", "ww", "vis", "weight"):
+        w[k] = np.asarray(inputs[k], dtype=np.float32)
+    w["cell_size_rad"] = float(np.float32(inputs["cell_size_rad"]))
+    w["w_scale"] = float(np.float32(inputs["w_scale"]))
+    g = w["grid_size"]
+    ns, npl = O.diagnostics_sizes(w)
+    init = dict(grid=rng.normal(size=2 * g * g).astype(np.float32),
+                norm=0.5,
+                num_vis_per_wsupport=rng.integers(0, 5, ns).astype(np.int64),
+                num_vis_per_wplane=np.concatenate([
+                    rng.integers(0, 5, min(npl, 64)),
+                    np.zeros(max(0, npl - 64), np.int64)]).astype(np.int64),
+                num_vis_per_grid=rng.integers(0, 5, g * g).astype(np.int64),
+                avg_wsupport_per_grid=rng.integers(0, 50, g * g).astype(
+                    np.float32),
+                avg_wplane_per_grid=rng.uniform(size=g * g).astype(
+                    np.float32))
+    out = O.diagnostics_f(w, use_reference=True, init=init)
+    arrays = {k: w[k] for k in ("conv_func", "uu", "vv", "ww", "vis",
+                                "weight")}
+    np.savez_compressed(
+        os.path.join(OUT, name + ".npz"), support=inputs["support"],
+        num_w_planes=inputs["num_w_planes"], oversample=inputs["oversample"],
+        conv_size_half=inputs["conv_size_half"],
+        cell_size_rad=np.asarray(w["cell_size_rad"], dtype=np.float32),
+        w_scale=np.asarray(w["w_scale"], dtype=np.float32),
+        grid_size=g, single=True, **arrays,
+        **{"init_" + k: np.asarray(v) for k, v in init.items()},
+        **{"out_" + k: np.asarray(v) for k, v in out.items()})
+    print(f"{name}: n={len(w['uu'])} skipped={out['num_skipped']} "
+          f"planes hist={npl}")
+
+
 def main():
     save("edges_d", edge_case_inputs(), single=False)
     save("odd_oversample_d", odd_oversample_inputs(), single=False)
@@ -216,6 +257,7 @@ def main():
     save("ones_d", ones_inputs(), single=False)
     save_weights("weights_d", weights_inputs(), single=False)
     save_weights("weights_f", weights_inputs(), single=True)
+    save_diagnostics("diag_edges_f", edge_case_inputs())
 
 
 if __name__ == "__main__":

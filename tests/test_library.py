@@ -64,6 +64,27 @@ def test_drop_in_signatures_match_reference_header():
             f"{real}* grid"]
 
 
+def test_diagnostics_signature_matches_reference_definition():
+    """Same parameter list as oskar_grid_wproj_f_diagnostics
+    (oskar_grid_wproj.c:245-267), which no reference header declares."""
+    text = open(os.path.join(ROOT, "include",
+                             "oskar_grid_wproj_b200.h")).read()
+    m = re.search(r"void oskar_grid_wproj_f_diagnostics\((.*?)\);", text,
+                  re.S)
+    params = [" ".join(p.split()) for p in m.group(1).split(",")]
+    assert params == [
+        "const size_t num_w_planes", "const int* support",
+        "const int oversample", "const int conv_size_half",
+        "const float* conv_func", "const size_t num_points",
+        "const float* uu", "const float* vv", "const float* ww",
+        "const float* vis", "const float* weight",
+        "const float cell_size_rad", "const float w_scale",
+        "const int grid_size", "size_t* num_skipped", "double* norm",
+        "float* grid", "long long int* num_vis_per_wsupport",
+        "long long int* num_vis_per_wplane", "long long int* num_vis_per_grid",
+        "float* avg_wsupport_per_grid", "float* avg_wplane_per_grid"]
+
+
 def _has_sm100():
     try:
         import torch
@@ -88,6 +109,26 @@ def test_drop_in_fails_loudly_without_a_device():
                               grid)
     assert e.value.status == _lib.ERR_NO_DEVICE
     assert (grid == 7.0).all()
+
+
+@pytest.mark.skipif(_has_sm100(), reason="a B200 is present")
+def test_diagnostics_fails_loudly_without_a_device():
+    """No GPU: the diagnostics drop-in reports NO_DEVICE and leaves every
+    output alone."""
+    g = 8
+    grid = np.full(2 * g * g, 7.0, np.float32)
+    counts = [np.full(2, 3, np.int64), np.full(2, 3, np.int64),
+              np.full(g * g, 3, np.int64)]
+    avg = np.full(g * g, 2.0, np.float32)
+    pts = np.zeros(3, np.float32)
+    with pytest.raises(fg.GridderError) as e:
+        fg.oskar_grid_wproj_f_diagnostics(
+            1, np.array([1], np.int32), 4, 7, np.ones(98, np.float32), 3,
+            pts, pts, pts, np.zeros(6, np.float32), None, 1.0 / g, 1.0, g,
+            5.0, grid, *counts, avg, None)
+    assert e.value.status == _lib.ERR_NO_DEVICE
+    assert (grid == 7.0).all() and (avg == 2.0).all()
+    assert all((c == 3).all() for c in counts)
 
 
 def test_invalid_arguments_rejected_before_any_device_work():

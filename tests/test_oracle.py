@@ -256,3 +256,52 @@ def test_weighted_oracle_scales_each_visibility(oracle):
     _, n_two, _ = oracle.grid_weighted_d(two)
     _, n_one, _ = oracle.grid_d(w)
     assert n_two == 2.0 * n_one
+
+
+def _diag_equal(a, b):
+    for k in ("grid", "num_vis_per_wsupport", "num_vis_per_wplane",
+              "num_vis_per_grid", "avg_wsupport_per_grid",
+              "avg_wplane_per_grid"):
+        assert np.array_equal(a[k], b[k]), k
+    assert a["norm"] == b["norm"]
+    assert a["num_skipped"] == b["num_skipped"]
+
+
+def test_diagnostics_oracle_matches_golden_bit_exact(oracle):
+    """oskar_grid_wproj_f_diagnostics (oskar_grid_wproj.c:245-370),
+    restated, against the reference's own outputs on the edge-case points
+    (skipped footprints, planes past the last one, half-way roundings) with
+    every in/out array starting from non-zero contents."""
+    from conftest import load_diag_golden
+    inputs, init, out = load_diag_golden("diag_edges_f")
+    _diag_equal(oracle.diagnostics_f(inputs, init=init), out)
+
+
+def test_diagnostics_oracle_matches_reference(oracle, ref, small):
+    part = dict(small)
+    for k in ("uu", "vv", "ww", "weight"):
+        part[k] = small[k][:30000]
+    part["vis"] = small["vis"][:60000]
+    _diag_equal(oracle.diagnostics_f(part),
+                oracle.diagnostics_f(part, use_reference=True))
+
+
+def test_diagnostics_grid_is_the_float_gridder(oracle, small):
+    """The diagnostics variant grids exactly as oskar_grid_wproj_f (without
+    its fixed 10000-point loop), and its counts add up: one count per point
+    in each histogram, one per tap of a kept point per cell."""
+    part = dict(small)
+    for k in ("uu", "vv", "ww", "weight"):
+        part[k] = small[k][:20000]
+    part["vis"] = small["vis"][:40000]
+    d = oracle.diagnostics_f(part)
+    s, n, g = oracle.grid_f(part)
+    assert d["num_skipped"] == s and d["norm"] == n
+    assert np.array_equal(d["grid"], g)
+    assert d["num_vis_per_wsupport"].sum() == 20000
+    assert d["num_vis_per_wplane"].sum() == 20000
+    p = oracle.place(part, single=True)
+    kept = p["skipped"] == 0
+    sup = np.asarray(part["support"])[p["plane"][kept]]
+    assert d["num_vis_per_grid"].sum() == int(((2 * sup + 1) ** 2).sum())
+    assert not d["avg_wplane_per_grid"].any()
