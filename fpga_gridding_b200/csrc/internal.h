@@ -340,7 +340,9 @@ int run_autotune(oskar_B200Workspace* ws, const oskar_B200Cube* cube,
                  double cell_size_rad, double w_scale, int grid_size,
                  void* grid, unsigned char* table_out);
 
-// dst[i] += src[i] for n reals (FP64 when is_double, else FP32).
+// dst[i] += src[i] for n reals (FP64 when is_double, else FP32); where
+// dst[i] is zero the result is src[i] itself (sign of zero and NaN bits
+// kept).
 cudaError_t launch_add(void* dst, const void* src, size_t n, int is_double,
                        int num_sms, cudaStream_t st);
 // *acc |= the workspace's device status word (after a run_batch on st).

@@ -535,13 +535,20 @@ __global__ void bounded_wait_probe_kernel(unsigned spins,
         atomicOr(status, (unsigned long long)DEV_ERR_TIMEOUT);
 }
 
+// dst = this call's contributions, src = the caller's values.  Where the
+// call added nothing (dst is zero) the caller's value is kept as it is, as
+// the reference leaves cells no footprint reaches (a -0.0 stays -0.0, a
+// NaN keeps its bits).
 template <typename T>
 __global__ void add_kernel(T* __restrict__ dst, const T* __restrict__ src,
                            size_t n)
 {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (size_t)gridDim.x * blockDim.x)
-        dst[i] += src[i];
+    {
+        const T a = dst[i], b = src[i];
+        dst[i] = a == T(0) ? b : a + b;
+    }
 }
 
 __global__ void status_or_kernel(const unsigned long long* counters,

@@ -120,6 +120,46 @@ def test_dropin_pipelined_chunks(oracle, single):
 
 
 @pytest.mark.parametrize("single", [False, True])
+def test_dropin_leaves_cells_no_footprint_reaches_bit_for_bit(oracle,
+                                                              single):
+    """Two clusters of points on a 512^2 grid.  Rows far from both hold
+    NaN and -0.0 in the caller's grid: they come back bit for bit, as the
+    reference never touches them (adding a zero contribution would turn
+    -0.0 into +0.0); the rest matches the oracle."""
+    rng = np.random.default_rng(31)
+    g, os_, n = 512, 4, 4000
+    support = W.support_ramp(8, 1, 3)
+    csh = W.min_conv_size_half(support, os_) + 1
+    cube = W.analytic_kernel_cube(support, os_, csh).numpy()
+    centre = np.where(np.arange(n) < n // 2, -156.0, 124.0)
+    pu = centre + rng.uniform(-20.0, 20.0, n)
+    pv = centre + rng.uniform(-20.0, 20.0, n)
+    w = dict(num_w_planes=8, support=support, oversample=os_,
+             conv_size_half=csh, conv_func=cube, uu=-pu / g, vv=pv / g,
+             ww=rng.uniform(-49.0, 49.0, n), vis=rng.normal(size=2 * n),
+             weight=np.ones(n), cell_size_rad=1.0, w_scale=1.0, grid_size=g)
+    real = np.float32 if single else np.float64
+    base = rng.normal(size=(g, g, 2)).astype(real)
+    base[250:262, :, 0] = np.nan
+    base[250:262, :, 1] = -0.0
+    base = base.reshape(-1)
+    special = np.zeros((g, g, 2), bool)
+    special[250:262] = True
+    special = special.reshape(-1)
+    ref_in = promote(w) if single else w
+    s1, n1, g1 = oracle.grid_d(ref_in, grid_arr=base.astype(np.float64),
+                               norm=0.0, threads=8)
+    s2, n2, g2 = fg.grid_workload(w, single=single, grid=base.copy(),
+                                  norm=0.0)
+    assert s1 == s2 == 0
+    assert np.array_equal(g2[special].view(np.uint8),
+                          base[special].view(np.uint8))
+    assert oracle.rel_rms(g2[~special], g1[~special]) <= \
+        (TOL_F if single else TOL_D)
+    assert abs(n2 - n1) <= TOL_D * abs(n1)
+
+
+@pytest.mark.parametrize("single", [False, True])
 def test_dropin_bands_wider_than_band_height(oracle, single):
     """Supports up to 70 on a 256^2 grid (bands of 64 rows): footprints
     reach past the neighbouring band, so a band's rows go back to the host
