@@ -263,7 +263,7 @@ int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
         B200_TRY(ws->rec.ensure(16 * n));
         if (!degrid)
         {
-            B200_TRY(ws->flags.ensure(4 * n));
+            B200_TRY(ws->flags.ensure(8 * task_tiles(n)));
             B200_TRY(ws->task_start.ensure(4 * (n + 2)));
             B200_TRY(ws->task_job.ensure(4 * (n + 2)));
         }
@@ -342,10 +342,10 @@ int run_batch(oskar_B200Workspace* ws, const oskar_B200Options* opt,
     B200_TRY(launch_tasks(keys[which], n, counters, 2 * kl.fine_bits,
                           kl.job_shift, kTaskMax,
                           static_cast<uint32_t*>(ws->flags.ptr),
-                          keys[which ^ 1], ws->scan_tmp.ptr,
+                          ws->scan_tmp.ptr,
                           static_cast<uint32_t*>(ws->task_start.ptr),
-                          static_cast<uint32_t*>(ws->task_job.ptr),
-                          ws->num_sms, st, &launches));
+                          static_cast<uint32_t*>(ws->task_job.ptr), st,
+                          &launches));
 
     GridArgs ga{};
     ga.order = vals[which];

@@ -247,47 +247,94 @@ __global__ void finalize_prep_kernel(const PrepArgs a)
     }
 }
 
-__global__ void task_flags_kernel(const uint32_t* __restrict__ keys, size_t n,
-                                  const unsigned long long* __restrict__ counters,
-                                  int fine_key_bits, int task_max,
-                                  uint32_t* __restrict__ flags)
+// Task list in two passes over the sorted keys, tiles of kTaskTile
+// positions: each tile counts its task starts, the tile counts are scanned,
+// and each tile writes its starts at its offset.  A task starts at sorted
+// position s < valid when s == 0, s % task_max == 0, or the key above the
+// fine cell bits changes.
+constexpr int kTaskTile = 4096;
+constexpr int kTaskThreads = 256;
+
+__device__ __forceinline__ bool task_starts_at(const uint32_t* keys, size_t s,
+                                               size_t valid, int fine_bits,
+                                               int task_max)
+{
+    return s < valid &&
+           (s == 0 || s % (size_t)task_max == 0 ||
+            (keys[s] >> fine_bits) != (keys[s - 1] >> fine_bits));
+}
+
+__global__ void __launch_bounds__(kTaskThreads)
+task_count_kernel(const uint32_t* __restrict__ keys, size_t n,
+                  const unsigned long long* __restrict__ counters,
+                  int fine_key_bits, int task_max,
+                  uint32_t* __restrict__ tile_counts)
 {
     const size_t valid = n - counters[CNT_SKIPPED];
-    for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < n;
-         s += (size_t)gridDim.x * blockDim.x)
+    const size_t tile0 = (size_t)blockIdx.x * kTaskTile;
+    unsigned c = 0;
+    for (int k = threadIdx.x; k < kTaskTile; k += kTaskThreads)
+        c += task_starts_at(keys, tile0 + k, valid, fine_key_bits, task_max);
+    c = warp_sum(c);
+    __shared__ unsigned s_w[kTaskThreads / 32];
+    if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0)
     {
-        uint32_t f = 0;
-        if (s < valid)
-        {
-            f = (s == 0) || (s % (size_t)task_max == 0) ||
-                ((keys[s] >> fine_key_bits) != (keys[s - 1] >> fine_key_bits));
-        }
-        flags[s] = f;
+        unsigned t = 0;
+        for (int w = 0; w < kTaskThreads / 32; ++w) t += s_w[w];
+        tile_counts[blockIdx.x] = t;
     }
 }
 
-__global__ void task_scatter_kernel(const uint32_t* __restrict__ flags,
-                                    const uint32_t* __restrict__ pos,
-                                    const uint32_t* __restrict__ keys, size_t n,
-                                    int job_shift,
-                                    unsigned long long* __restrict__ counters,
-                                    uint32_t* __restrict__ task_start,
-                                    uint32_t* __restrict__ task_job)
+// tile_offsets: exclusive scan of tile_counts (the last tile also needs its
+// own count to close the list).
+__global__ void __launch_bounds__(kTaskThreads)
+task_write_kernel(const uint32_t* __restrict__ keys, size_t n,
+                  unsigned long long* __restrict__ counters,
+                  int fine_key_bits, int task_max, int job_shift,
+                  const uint32_t* __restrict__ tile_counts,
+                  const uint32_t* __restrict__ tile_offsets,
+                  uint32_t* __restrict__ task_start,
+                  uint32_t* __restrict__ task_job)
 {
-    for (size_t s = (size_t)blockIdx.x * blockDim.x + threadIdx.x; s < n;
-         s += (size_t)gridDim.x * blockDim.x)
+    const size_t valid = n - counters[CNT_SKIPPED];
+    const size_t tile0 = (size_t)blockIdx.x * kTaskTile;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __shared__ unsigned s_w[kTaskThreads / 32];
+    uint32_t base = tile_offsets[blockIdx.x];
+    // rounds of kTaskThreads consecutive positions, in order
+    for (int r = 0; r < kTaskTile; r += kTaskThreads)
     {
-        if (flags[s])
+        const size_t pos = tile0 + r + threadIdx.x;
+        const bool f = task_starts_at(keys, pos, valid, fine_key_bits,
+                                      task_max);
+        const unsigned ball = __ballot_sync(0xffffffffu, f);
+        if (lane == 0) s_w[warp] = __popc(ball);
+        __syncthreads();
+        unsigned before = 0, total = 0;
+#pragma unroll
+        for (int w = 0; w < kTaskThreads / 32; ++w)
         {
-            task_start[pos[s]] = (uint32_t)s;
-            task_job[pos[s]] = keys[s] >> job_shift;
+            before += w < warp ? s_w[w] : 0u;
+            total += s_w[w];
         }
-        if (s == n - 1)
+        if (f)
         {
-            const uint32_t num_tasks = pos[s] + flags[s];
-            counters[CNT_TASKS] = num_tasks;
-            task_start[num_tasks] = (uint32_t)(n - counters[CNT_SKIPPED]);
+            const uint32_t t = base + before +
+                               __popc(ball & ((1u << lane) - 1u));
+            task_start[t] = (uint32_t)pos;
+            task_job[t] = keys[pos] >> job_shift;
         }
+        base += total;
+        __syncthreads();   // s_w is rewritten by the next round
+    }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0)
+    {
+        const uint32_t num_tasks = tile_offsets[blockIdx.x] +
+                                   tile_counts[blockIdx.x];
+        counters[CNT_TASKS] = num_tasks;
+        task_start[num_tasks] = (uint32_t)valid;
     }
 }
 
@@ -342,22 +389,26 @@ cudaError_t launch_finalize_prep(const PrepArgs& a, cudaStream_t st)
     return cudaGetLastError();
 }
 
+size_t task_tiles(size_t n) { return (n + kTaskTile - 1) / kTaskTile; }
+
 cudaError_t launch_tasks(const uint32_t* sorted_keys, size_t n,
                          unsigned long long* counters, int fine_key_bits,
-                         int job_shift, int task_max, uint32_t* flags,
-                         uint32_t* pos, void* scan_tmp, uint32_t* task_start,
-                         uint32_t* task_job, int num_sms, cudaStream_t st,
-                         int* launches)
+                         int job_shift, int task_max, uint32_t* tile_counts,
+                         void* scan_tmp, uint32_t* task_start,
+                         uint32_t* task_job, cudaStream_t st, int* launches)
 {
-    const unsigned blocks = grid_blocks(n, num_sms, 8, 256);
-    task_flags_kernel<<<blocks, 256, 0, st>>>(sorted_keys, n, counters,
-                                              fine_key_bits, task_max, flags);
-    cudaError_t e = exclusive_scan_u32(flags, pos, n, scan_tmp, st, launches);
+    const size_t tiles = task_tiles(n);
+    if (tiles == 0) return cudaSuccess;
+    uint32_t* tile_offsets = tile_counts + tiles;
+    task_count_kernel<<<(unsigned)tiles, kTaskThreads, 0, st>>>(
+        sorted_keys, n, counters, fine_key_bits, task_max, tile_counts);
+    cudaError_t e = exclusive_scan_u32(tile_counts, tile_offsets, tiles,
+                                       scan_tmp, st, launches);
     if (e != cudaSuccess) return e;
     if (launches) *launches += 2;
-    task_scatter_kernel<<<blocks, 256, 0, st>>>(flags, pos, sorted_keys, n,
-                                                job_shift, counters,
-                                                task_start, task_job);
+    task_write_kernel<<<(unsigned)tiles, kTaskThreads, 0, st>>>(
+        sorted_keys, n, counters, fine_key_bits, task_max, job_shift,
+        tile_counts, tile_offsets, task_start, task_job);
     return cudaGetLastError();
 }
 

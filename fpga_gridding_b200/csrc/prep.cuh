@@ -141,13 +141,15 @@ cudaError_t launch_prep(const PrepArgs& a, int data_is_double, int coord_mode,
 // Per job: norm += sum of its partials; skip count; grid updates.
 cudaError_t launch_finalize_prep(const PrepArgs& a, cudaStream_t st);
 // Task list: a task starts where (job, coarse tile, plane) changes and every
-// task_max positions; task_job[t] is the job of task t.
+// task_max positions; task_job[t] is the job of task t.  tile_counts holds
+// 2 * task_tiles(n) entries; scan_tmp as exclusive_scan_u32 needs for
+// task_tiles(n) values.
+size_t task_tiles(size_t n);
 cudaError_t launch_tasks(const uint32_t* sorted_keys, size_t n,
                          unsigned long long* counters, int fine_key_bits,
-                         int job_shift, int task_max, uint32_t* flags,
-                         uint32_t* pos, void* scan_tmp, uint32_t* task_start,
-                         uint32_t* task_job, int num_sms, cudaStream_t st,
-                         int* launches);
+                         int job_shift, int task_max, uint32_t* tile_counts,
+                         void* scan_tmp, uint32_t* task_start,
+                         uint32_t* task_job, cudaStream_t st, int* launches);
 // Bands of a single job's task list: band b holds the tasks of coarse-tile
 // row b; band_first[b] (b <= num_bands) is its first task.
 cudaError_t launch_band_first(const uint32_t* sorted_keys,

@@ -77,9 +77,9 @@ struct Slot
 // Workspace bytes a batch of n points needs (run_batch's buffers).
 size_t workspace_need(size_t n)
 {
-    // keys and indices (twice), records, task flags, starts and jobs, and
-    // the sort's scratch: 48 bytes per point in either precision
-    return n * 48u + (8u << 20);
+    // keys and indices (twice), records, task starts and jobs, and the
+    // sort's scratch: 44 bytes per point in either precision
+    return n * 44u + (8u << 20);
 }
 
 }  // namespace

@@ -39,7 +39,7 @@ int static_cube_fill(const float* d_conv, int num_planes, int oversample,
 
 namespace {
 
-// 64 MiB: about 1.4 million visibilities with a small cube (~45 bytes of
+// 64 MiB: about 1.5 million visibilities with a small cube (~41 bytes of
 // scratch per visibility plus the re-laid cube).
 constexpr size_t kStaticScratchBytes = size_t(64) << 20;
 constexpr int kMaxDevices = 64;
@@ -149,7 +149,7 @@ extern "C" int oskar_b200_grid_f_static(
     uint32_t* keys[2] = {cv.take<uint32_t>(4 * n), cv.take<uint32_t>(4 * n)};
     uint32_t* vals[2] = {cv.take<uint32_t>(4 * n), cv.take<uint32_t>(4 * n)};
     auto* rec = cv.take<int4>(16 * n);
-    auto* flags = cv.take<uint32_t>(4 * n);
+    auto* tile_counts = cv.take<uint32_t>(8 * task_tiles(n));
     auto* task_start = cv.take<uint32_t>(4 * (n + 2));
     auto* task_job = cv.take<uint32_t>(4 * (n + 2));
     const size_t tmp = std::max(radix_sort_temp_bytes(n > 0 ? n : 1),
@@ -233,8 +233,8 @@ extern "C" int oskar_b200_grid_f_static(
     B200_S(radix_sort_pairs(keys, vals, n, kl.total_bits + 1, scan_tmp, s,
                             &which, nullptr));
     B200_S(launch_tasks(keys[which], n, counters, 2 * kl.fine_bits,
-                        kl.job_shift, kTaskMax, flags, keys[which ^ 1],
-                        scan_tmp, task_start, task_job, num_sms, s, nullptr));
+                        kl.job_shift, kTaskMax, tile_counts, scan_tmp,
+                        task_start, task_job, s, nullptr));
     GridArgs ga{};
     ga.order = vals[which];
     ga.rec = rec;

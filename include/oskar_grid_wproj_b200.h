@@ -519,7 +519,7 @@ OSKAR_B200_EXPORT int oskar_b200_measure_atomic_rate(oskar_B200Workspace* ws,
  * are device pointers; support is host memory; weight is ignored as in the
  * reference.  All scratch (the re-laid cube, sort keys, records, task list)
  * comes from one static device array of 64 MiB that every GPU loading this
- * library holds until the process exits: enough for about 1.4 million
+ * library holds until the process exits: enough for about 1.5 million
  * visibilities with a small cube.  A job that does not fit returns
  * OSKAR_B200_ERR_OVER_BUDGET and touches nothing.  The array's device
  * address is looked up on the first call on each device (with that device

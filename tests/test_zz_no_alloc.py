@@ -117,7 +117,7 @@ def test_static_entry_refuses_jobs_beyond_its_scratch(job):
     grid = torch.zeros(2 * job["g"] ** 2, device="cuda")
     skip = torch.zeros(1, dtype=torch.int64, device="cuda")
     norm = torch.zeros(1, dtype=torch.float64, device="cuda")
-    # 4 million points need ~180 MB of scratch: refused before any device
+    # 4 million points need ~165 MB of scratch: refused before any device
     # work (the pointers are never read)
     st = _static_call(lib, job, grid, skip, norm, n=4_000_000)
     assert st == _lib.ERR_OVER_BUDGET
