@@ -1,8 +1,8 @@
 // Per-visibility preparation of a batch of jobs: placement (grid cell,
 // w-plane, oversample offsets, conjugation, skip test) exactly as
 // oskar_grid_wproj.c:70-101 computes it, the sort key, the skip counts, the
-// norms and the plane histograms; then, after the sort, the permutation into
-// sorted order and the gridding work list (tasks).
+// norms and the plane histograms; then, after the sort, the gridding work
+// list (tasks).
 #include <algorithm>
 
 #include "common.cuh"
