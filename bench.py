@@ -95,10 +95,11 @@ def measured_peaks():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def profiled_value(key):
-    """A per-launch figure of the gridding kernel from the committed ncu
-    summary (profiles/romein_grid_kernel_plain_large.md), or None."""
-    p = os.path.join(ROOT, "profiles", "romein_grid_kernel_plain_large.md")
+def profiled_value(key, profile="romein_grid_kernel_plain_large.md"):
+    """A per-launch figure from a committed ncu summary (by default the
+    gridding kernel's, profiles/romein_grid_kernel_plain_large.md), or
+    None."""
+    p = os.path.join(ROOT, "profiles", profile)
     try:
         text = open(p).read()
     except OSError:
@@ -1254,10 +1255,23 @@ def run_degrid(args, world, rank, local):
                         "sort": round(st.sort_ms, 3),
                         "degrid": round(st.grid_ms, 3)},
            "roofline": {"kernel": "degrid_kernel<float,float2>",
-                        "bound": "hbm", "achieved": round(achieved, 2),
+                        "bound": "issue",
+                        "bound_evidence": "ncu: L1 loads of kernel values "
+                                          "and grid cells and instruction "
+                                          "issue limit it; DRAM throughput "
+                                          "about 5 %",
+                        "achieved": round(achieved, 2),
                         "peak": peak, "peak_source": peak_kind,
                         "unit": "GB/s", "frac": round(achieved / peak, 4),
-                        "traffic": None,
+                        "traffic": profiled_value(
+                            "dram_bytes_per_launch_full_job",
+                            "degrid_kernel_plain_large.md"),
+                        "traffic_source": "ncu dram__bytes_read.sum + "
+                                          "dram__bytes_write.sum of one "
+                                          "full-size launch, copied from "
+                                          "profiles/degrid_kernel_plain_"
+                                          "large.md (not measured in this "
+                                          "run)",
                         "algorithmic_bytes_per_launch": alg,
                         "kernel_ms": round(kernel_ms, 3)},
            "gpu_launches": launches, "skipped": int(skip.item()),
