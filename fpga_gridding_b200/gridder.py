@@ -79,6 +79,26 @@ def oskar_grid_wproj_f_diagnostics(num_w_planes, support, oversample,
     (num_skipped, norm)."""
     lib = load()
     support = np.ascontiguousarray(support, dtype=np.int32)
+    # The library writes as many entries as the reference's indexing needs;
+    # refuse arrays too small for them instead of letting it write past
+    # their ends.  The largest plane index in the float arithmetic:
+    # roundf(sqrtf(|w * w_scale|)), half away from zero.
+    cells = grid_size * grid_size
+    if num_points:
+        r = np.sqrt(np.abs(np.asarray(ww, np.float32)[:num_points] *
+                           np.float32(w_scale)))
+        plane_max = int(np.floor(r.astype(np.float64) + 0.5).max())
+    else:
+        plane_max = -1
+    for arr, need, name in (
+            (num_vis_per_wsupport, int(support.max()) + 1,
+             "num_vis_per_wsupport"),
+            (num_vis_per_wplane, plane_max + 1, "num_vis_per_wplane"),
+            (num_vis_per_grid, cells, "num_vis_per_grid"),
+            (avg_wsupport_per_grid, cells, "avg_wsupport_per_grid")):
+        if np.asarray(arr).size < need:
+            raise ValueError(f"{name} holds {np.asarray(arr).size} entries; "
+                             f"this call needs {need}")
     skipped = C.c_size_t(0)
     nrm = C.c_double(norm)
     fn = lib.oskar_grid_wproj_f_diagnostics

@@ -131,6 +131,26 @@ def test_diagnostics_fails_loudly_without_a_device():
     assert all((c == 3).all() for c in counts)
 
 
+def test_diagnostics_wrapper_refuses_arrays_too_small():
+    """The Python wrapper checks the count arrays against the entries the
+    reference's indexing needs (largest unclamped plane index in float
+    arithmetic) before the library could write past them."""
+    g = 8
+    ww = np.array([0.0, 24.5, 3.9], np.float32)   # planes 0, 5 (4.95), 2
+    pts = np.zeros(3, np.float32)
+    args = (1, np.array([1], np.int32), 4, 7, np.ones(98, np.float32), 3,
+            pts, pts, ww, np.zeros(6, np.float32), None, 1.0 / g, 1.0, g,
+            0.0, np.zeros(2 * g * g, np.float32))
+    with pytest.raises(ValueError, match="num_vis_per_wplane"):
+        fg.oskar_grid_wproj_f_diagnostics(
+            *args, np.zeros(2, np.int64), np.zeros(5, np.int64),
+            np.zeros(g * g, np.int64), np.zeros(g * g, np.float32), None)
+    with pytest.raises(ValueError, match="num_vis_per_grid"):
+        fg.oskar_grid_wproj_f_diagnostics(
+            *args, np.zeros(2, np.int64), np.zeros(6, np.int64),
+            np.zeros(g * g - 1, np.int64), np.zeros(g * g, np.float32), None)
+
+
 def test_invalid_arguments_rejected_before_any_device_work():
     lib = fg.load()
     skipped = C.c_size_t(99)
