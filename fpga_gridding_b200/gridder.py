@@ -83,13 +83,16 @@ def oskar_grid_wproj_f_diagnostics(num_w_planes, support, oversample,
     # refuse arrays too small for them instead of letting it write past
     # their ends.  The largest plane index in the float arithmetic:
     # roundf(sqrtf(|w * w_scale|)), half away from zero.
+    # (Indices that are not finite or not below 2^24 make the library refuse
+    # the call before it writes anything.)
     cells = grid_size * grid_size
+    plane_max = -1
     if num_points:
         r = np.sqrt(np.abs(np.asarray(ww, np.float32)[:num_points] *
                            np.float32(w_scale)))
-        plane_max = int(np.floor(r.astype(np.float64) + 0.5).max())
-    else:
-        plane_max = -1
+        top = np.floor(r.astype(np.float64) + 0.5).max()
+        if np.isfinite(top) and top < 2 ** 24:
+            plane_max = int(top)
     for arr, need, name in (
             (num_vis_per_wsupport, int(support.max()) + 1,
              "num_vis_per_wsupport"),
